@@ -1,0 +1,417 @@
+#!/usr/bin/env python
+"""bench.py -- FD Mcell-updates/s and HBM roofline fraction on one B200 node.
+
+Workload (default, the batched-RTM configuration): 201^3 model at 10 m, five
+layers plus -8 %/+12 % Gaussian anomalies, smoothed migration model, 50-cell
+random boundary (301^3 padded cells), nt = 2001 at 1 ms, Ricker 10 Hz peak
+(N = 2120 time steps), 64 shots on an 8 x 8 grid with clipped 121 x 121
+receiver patches.  One step = one shot's full RTM: new random boundary,
+forward propagation, then the fused pass (source rebuilt backwards + adjoint
+propagation + imaging), 3 padded cells x N steps of cell-updates.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload rtm|modeling]
+
+Multi-GPU: one process per GPU (torchrun); shots are dealt round-robin to
+ranks (weak scaling) and the images are summed with one NCCL all-reduce at
+the end of the timed region; time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+MEASURED = ROOT / "MEASURED_PEAKS.json"
+TRAFFIC = ROOT / "profiles" / "traffic.json"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def hbm_peak():
+    try:
+        return float(json.loads(MEASURED.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 8:
+                continue
+            try:
+                sm.append(float(p[0]))
+                mx = float(p[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def workload(name):
+    from fwi3d_b200 import synth
+    if name == "rtm":
+        return synth.rtm_201()
+    if name == "modeling":
+        return synth.modeling_101()
+    raise SystemExit(f"unknown workload {name}")
+
+
+def cpu_baseline(w, n_steps=40):
+    """FP64 oracle (OpenMP, all host cores) on a bounded sample of the same
+    workload: n_steps forward + n_steps fused backward steps on the full padded
+    grid.  Returns Mcell-updates/s."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+    v = w.start if w.start is not None else w.vp
+    vpp = orc.expand(v, w.nz, w.nx, w.ny, w.nb)
+    nyy, nxx, nzz = vpp.shape
+    wl, _ = orc.wavelet(n_steps, w.dt, w.fmax)
+    src = orc.flat_index(nzz // 2, nxx // 2, nyy // 2, nzz, nxx)
+    rec = np.array([src + 1], np.int64)
+    t0 = time.perf_counter()
+    _, P, Q = orc.forward(vpp, w.dh, w.dt, n_steps, 0, wl, src, rec)
+    t1 = time.perf_counter()
+    orc.backward(vpp, w.dh, w.dt, n_steps, 0, rec, np.zeros((1, n_steps)), P, Q)
+    t2 = time.perf_counter()
+    cells = nzz * nxx * nyy
+    updates = cells * n_steps * 3
+    return {"value": updates / (t2 - t0) / 1e6, "unit": "Mcell-updates/s", "cores": orc.num_threads(),
+            "kind": "port",
+            "sample": f"FP64 oracle, {n_steps} forward + {n_steps} fused backward steps on the "
+                      f"{nzz}x{nxx}x{nyy} padded grid ({t2 - t0:.1f} s)"}
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    from fwi3d_b200 import lib
+
+    w = workload(args.workload)
+    rtm = args.workload == "rtm"
+    boundary = lib.BOUNDARY_RBC
+    ctx = lib.Context(w.nz, w.nx, w.ny, w.nb, w.dh, w.nt, w.dt, w.fmax, boundary, w.abc_factor, 1, 0)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_geometry(w.src, w.rec, w.rec_first, w.rec_count)
+    ctx.set_velocity(w.start if w.start is not None else w.vp)
+    ctx.autotune()
+    nsrc = len(w.src)
+    N = ctx.tlag + w.nt
+    cells = ctx.nzz * ctx.nxx * ctx.nyy
+    updates_per_step = cells * N * (3 if rtm else 1)
+
+    total = args.warmup + args.steps
+    shots = [(rank + ws * k) % nsrc for k in range(total)]
+    g = torch.Generator(device="cuda").manual_seed(1234 + rank)
+    data = {}
+    if rtm:
+        for s in set(shots):
+            data[s] = torch.randn(ctx.shot_nrec(s) * w.nt, generator=g, device="cuda", dtype=torch.float32)
+    seis_dev = None
+    if not rtm:
+        seis_dev = torch.empty(max(ctx.shot_nrec(s) for s in range(nsrc)) * w.nt, device="cuda")
+    rbc = dict(w.rbc)
+
+    def step(s, timing):
+        ctx.apply_random_boundary(seed=1000 + s, **rbc)
+        if rtm:
+            ctx.rtm_shots_dev([s], data[s].data_ptr())
+        else:
+            ctx.model_shots_dev([s], seis_dev.data_ptr())
+        f, b = ctx.last_timing()
+        timing[0] += f
+        timing[1] += b
+
+    tw = [0.0, 0.0]
+    for k in range(args.warmup):
+        step(shots[k], tw)
+    torch.cuda.synchronize()
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = ctx.launch_count()
+    timing = [0.0, 0.0]
+    img_all = ill_all = None
+    if ws > 1 and rtm:
+        img_all = torch.empty(cells, device="cuda")
+        ill_all = torch.empty(cells, device="cuda")
+    with ClockSampler(local) as clocks:
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for k in range(args.warmup, total):
+                step(shots[k], timing)
+            if img_all is not None:
+                import torch.distributed as dist
+                ctx.get_accumulators_dev(img_all.data_ptr(), ill_all.data_ptr())
+                dist.all_reduce(img_all)
+                dist.all_reduce(ill_all)
+                ctx.set_accumulators_dev(img_all.data_ptr(), ill_all.data_ptr())
+            e1.record(stream)
+        torch.cuda.synchronize()
+    launches = ctx.launch_count() - launches0
+    barrier(ws)
+    ms_local = e0.elapsed_time(e1)
+    ms = max_over_ranks(ms_local, ws)
+    value = updates_per_step * args.steps * ws / (ms / 1e3) / 1e6
+
+    # roofline of the dominant kernel: the fused backward step (44 B per
+    # cell-step) for RTM, the forward step (16 B per cell-update) for modeling
+    peak, peak_kind = hbm_peak()
+    if rtm:
+        kern_ms = timing[1] / args.steps / N
+        bytes_per_launch = 44.0 * cells
+        name = "fd_backward_kernel"
+    else:
+        kern_ms = timing[0] / args.steps / N
+        bytes_per_launch = 16.0 * cells
+        name = "fd_forward_kernel"
+    achieved = bytes_per_launch / (kern_ms / 1e3) / 1e9
+    traffic = None
+    try:
+        tr = json.loads(TRAFFIC.read_text())
+        if name in tr:
+            traffic = float(tr[name]["bytes_per_cell"]) * cells
+    except Exception:
+        pass
+    fwd_ms = timing[0] / args.steps / N
+    roof = {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+            "traffic": traffic, "algorithmic_bytes": bytes_per_launch,
+            "launch_ms": round(kern_ms, 5),
+            "forward_kernel": {"achieved": round(16.0 * cells / (fwd_ms / 1e3) / 1e9, 1),
+                               "frac": round(16.0 * cells / (fwd_ms / 1e3) / 1e9 / peak, 4),
+                               "launch_ms": round(fwd_ms, 5)}}
+
+    # end to end through the public API with host buffers
+    e2e = None
+    if rank == 0 or ws > 1:
+        host = {}
+        for s in set(shots[args.warmup:]):
+            n = (ctx.shot_nrec(s) * w.nt)
+            pin = torch.empty(n, dtype=torch.float32, pin_memory=True)
+            if rtm:
+                pin.copy_(data[s].cpu())
+            host[s] = pin
+        out = torch.empty(w.nz * w.nx * w.ny if rtm else max(ctx.shot_nrec(s) for s in range(nsrc)) * w.nt,
+                          dtype=torch.float32, pin_memory=True)
+        h2d = d2h = 0
+        barrier(ws)
+        t0 = time.perf_counter()
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for k in range(args.warmup, total):
+                s = shots[k]
+                ctx.apply_random_boundary(seed=1000 + s, **rbc)
+                if rtm:
+                    ctx.rtm_shots([s], host[s].numpy())
+                    out.numpy()[:] = ctx.rtm_image().ravel()
+                    h2d += host[s].numel() * 4
+                    d2h += out.numel() * 4
+                else:
+                    r = ctx.model_shots([s])[0]
+                    d2h += r.size * 4
+            e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1), ws)
+        wall = time.perf_counter() - t0
+        e2e = {"value": round(updates_per_step * args.steps * ws / (e2e_ms / 1e3) / 1e6, 1),
+               "unit": "Mcell-updates/s", "h2d_bytes_per_step": h2d // args.steps,
+               "d2h_bytes_per_step": d2h // args.steps, "wall_s": round(wall, 3)}
+
+    if rank != 0:
+        return None
+    line = {
+        "metric": "FD Mcell-updates/s", "value": round(value, 1), "unit": "Mcell-updates/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded layered model with Gaussian anomalies, seeded random observed data",
+        "config": {
+            "workload": (f"{w.name}: padded {ctx.nzz}x{ctx.nxx}x{ctx.nyy}, nt={w.nt}, N={N} steps; "
+                         + ("one shot per step: random boundary + forward + fused backward (3 cell-updates "
+                            "per padded cell per step)" if rtm else "one shot per step: forward modeling")),
+            "shots": nsrc, "l2": "inputs larger than L2 (every field 110 MB; 7 fields per shot)",
+            "tiles": ctx.tiles(), "parallelism": f"shots/{ws}"},
+        "roofline": roof,
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+    }
+    return line, clocks.summary()
+
+
+def run_reference(args, ws, rank, local):
+    """The reference's own CUDA build (oracle/_ref, compiled from its sources)
+    on the same workload: per step, Modeling::forward_solver plus the
+    Migration::backward_propagation loop of inject_seismogram +
+    cross_correlation, timed with CUDA events around the two time loops."""
+    if rank != 0:
+        return None
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+    if not orc.ref_available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libref_fwi3d.so was not built "
+                "(reference sources absent when building)"}, None
+    w = workload(args.workload)
+    rtm = args.workload == "rtm"
+    v = w.start if w.start is not None else w.vp
+    vpp = orc.expand(v, w.nz, w.nx, w.ny, w.nb).astype(np.float32)
+    nyy, nxx, nzz = vpp.shape
+    # the same kind of pad as ours, generated host-side (ramped +-30 %)
+    sys.path.insert(0, str(ROOT / "tests" / "golden"))
+    nb = w.nb
+
+    def ramp(n):
+        i = np.arange(n)
+        d = np.where(i < nb, nb - i, np.where(i >= n - nb, i - (n - nb - 1), 0))
+        return d / nb
+
+    r = np.maximum(np.maximum(ramp(nyy)[:, None, None], ramp(nxx)[None, :, None]), ramp(nzz)[None, None, :])
+    vpp = (vpp * (1 + 0.3 * r * np.random.default_rng(5).uniform(-1, 1, vpp.shape))).astype(np.float32)
+    lim = 0.98 * 2 / np.sqrt(3 * 6.501) * w.dh / w.dt
+    vpp = np.minimum(vpp, lim).astype(np.float32)
+    nsrc = len(w.src)
+    total = args.warmup + args.steps
+    shots = [k % nsrc for k in range(total)]
+    tmp = tempfile.mkdtemp()
+    cells = nzz * nxx * nyy
+    ms_sum = 0.0
+    N = None
+    with ClockSampler(local) as clocks:
+        for k, s in enumerate(shots):
+            f, c = (w.rec_first[s], w.rec_count[s]) if w.rec_first is not None else (0, len(w.rec))
+            rec = w.rec[f:f + c]
+            params = orc.write_reference_setup(Path(tmp) / f"s{k}", w.nz, w.nx, w.ny, w.dh, w.nt, w.dt, w.fmax,
+                                               w.nb, w.src[s:s + 1], rec)
+            adj = np.random.default_rng(s).standard_normal((len(rec), w.nt)).astype(np.float32) if rtm else None
+            out = orc.ref_run(params, vpp, shot=0, abc=not rtm, backward=1 if rtm else 0, adj=adj)
+            N = out["tlag"] + w.nt
+            if k >= args.warmup:
+                ms_sum += float(out["ms"][0] + out["ms"][1])
+    updates = cells * N * (3 if rtm else 1) * args.steps
+    value = updates / (ms_sum / 1e3) / 1e6
+    line = {"impl": "reference", "metric": "FD Mcell-updates/s", "value": round(value, 1),
+            "unit": "Mcell-updates/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms_sum / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 storage, f64 stencil arithmetic", "data": "synthetic",
+            "config": {"workload": f"{w.name}: padded {nzz}x{nxx}x{nyy}, nt={w.nt}, N={N}; reference CUDA "
+                                   "build (sm_100a) of FWI3D's own kernels, device time of its time loops"},
+            "cpu_baseline": {"value": round(value, 1), "unit": "Mcell-updates/s", "cores": 0,
+                             "kind": "reference",
+                             "sample": "reference CUDA build on the GPU (the reference has no CPU path)"},
+            "e2e": {"value": round(value, 1), "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    return line, clocks.summary()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["rtm", "modeling"], default="rtm")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    ws, rank, local = dist_setup()
+    if args.impl == "reference":
+        res = run_reference(args, ws, rank, local)
+    else:
+        res = run_ours(args, ws, rank, local)
+    if rank == 0 and res is not None:
+        line, clocks = res
+        if clocks is not None:
+            line["clocks"] = clocks
+        if args.impl == "ours" and ws == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(workload(args.workload))
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

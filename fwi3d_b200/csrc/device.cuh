@@ -1,0 +1,200 @@
+// device.cuh -- PTX helpers (TMA, mbarrier), constants and argument structs
+// shared by the stencil kernels.  sm_100a only.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fwi {
+
+// 8th-order second-derivative weights, FP32 images of the reference's double
+// literals (src/modeling/modeling.cuh:9-13): centre, then taps m = 1..4.
+// The operator is  -W0 f0 + W1 (f1+f-1) - W2 (f2+f-2) + W3 (f3+f-3) - W4 (f4+f-4).
+constexpr float W0 = 2.847222222222f;
+constexpr float W1 = 1.600000000000f;
+constexpr float W2 = 0.200000000000f;
+constexpr float W3 = 0.025396825396f;
+constexpr float W4 = 0.001785714285f;
+
+constexpr int kMaxBatch = 64;      // shots per launch
+constexpr int kMaxPad = 1024;      // largest pad width the damper table holds
+constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s cap on any device wait
+
+// Error bits the kernels raise in g_status (read back by the host).
+constexpr unsigned kErrTimeout = 1u;
+
+// Per-batch shot description, device resident so that a captured time loop
+// can be replayed for any batch of shots without re-capture.
+struct BatchInfo {
+    int nshot;                    // shots in this batch
+    int R;                        // receivers of all shots together
+    int ncell;                    // distinct receiver cells of all shots together
+    int pad_;
+    int src[kMaxBatch][3];        // source cell (i=z, j=x, k=y), padded indices
+};
+
+// Forward step arguments (one leapfrog step of every shot of a batch).
+struct FwdArgs {
+    int nzz, nxx, nyy, ldz;
+    long long vol;                // device elements of one shot's field (pitched)
+    int ntz, ntx, ylen;           // z tiles, x tiles, planes per y chunk
+    int t, nt, tlag;              // step index, wavelet length, recording lag
+    float cvel;                   // dt^2 / dh^2
+    float idh3;                   // source / adjoint scaling 1/dh^3
+    int nb;                       // pad width (damper tables)
+    float *Q;                     // field written this step (batch base)
+    const float *A;               // field read with the stencil (batch base)
+    const float *b1d;             // Cerjan 1-D table (ABC only)
+    const float *wavelet;         // [nt]
+    const BatchInfo *binfo;
+    const long long *rec_cell;    // [R] batch-flat cell index of each receiver
+    const float *rec_damp;        // [R] damping at the receiver (1 without ABC)
+    float *seis_tm;               // [nt][R] time-major seismograms
+};
+
+// Fused backward step arguments (source rebuild + adjoint + imaging).
+struct BwdArgs {
+    int nzz, nxx, nyy, ldz;
+    long long vol;
+    int ntz, ntx, ylen;
+    int t, nt, nsteps;            // backward step index, wavelet length, N = nt + tlag
+    float cvel;                   // dt^2 / dh^2
+    float gscale;                 // dt / dh^2 (gradient imaging condition)
+    float idh3;
+    int subtract_src;             // remove the source while rebuilding Ps
+    float *Ps;                    // rebuilt source field (written)
+    const float *Psold;           // source field read with the stencil
+    float *Prold;                 // adjoint field written
+    const float *Pr;              // adjoint field read with the stencil
+    float *image;                 // image or gradient accumulator (batch base)
+    float *illum;                 // illumination accumulator (batch base)
+    const float *wavelet;
+    const BatchInfo *binfo;
+};
+
+// ---------------------------------------------------------------------------
+// PTX wrappers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_addr(const void *p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Wait for phase `parity` of an mbarrier, giving up after kWaitLimitNs.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (;;) {
+#pragma unroll 1
+        for (int i = 0; i < 32; ++i)
+            if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > kWaitLimitNs) return false;
+    }
+}
+
+// 4-D tiled TMA load (z, x, y, shot) into shared memory, completing on bar.
+// No multicast: every CTA fetches its own tiles from this GPU's memory.
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, uint64_t *bar,
+                                            int c0, int c1, int c2, int c3)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4, %5, %6}], [%2];" ::"r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_addr(bar)), "r"(c0), "r"(c1), "r"(c2),
+        "r"(c3)
+        : "memory");
+}
+
+__device__ __forceinline__ void prefetch_tmap(const CUtensorMap *map)
+{
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+}
+
+__device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+
+__device__ __forceinline__ float comp(const float4 &v, int e)
+{
+    return e == 0 ? v.x : (e == 1 ? v.y : (e == 2 ? v.z : v.w));
+}
+
+__device__ __forceinline__ void set_comp(float4 &v, int e, float s)
+{
+    if (e == 0) v.x = s;
+    else if (e == 1) v.y = s;
+    else if (e == 2) v.z = s;
+    else v.w = s;
+}
+
+// Distance into the pad along one axis, -1 inside (src/modeling/modeling.cu:408-431).
+__device__ __forceinline__ int pad_depth(int i, int n, int nb)
+{
+    return i < nb ? i : (i >= n - nb ? n - 1 - i : -1);
+}
+
+// Cerjan factor of a cell from the 1-D table, bit-identical to the reference's
+// b2d/b3d tables (src/modeling/modeling.cu:101-127): the 2-D entry is
+// (b1[a] + b1[b]) - 1 and the 3-D entry ((B(z,x) + B(x,y)) + B(z,y)) - 5 with
+// B(p,q) = b1[p] + b1[q], all in FP32 in that order.
+__device__ __forceinline__ float cerjan(const float *b1, int dz, int dx, int dy)
+{
+    const int n = (dz >= 0) + (dx >= 0) + (dy >= 0);
+    if (n == 0) return 1.0f;
+    if (n == 1) return b1[dz >= 0 ? dz : (dx >= 0 ? dx : dy)];
+    if (n == 2) {
+        const int u = dz >= 0 ? dz : dx;
+        const int v = dy >= 0 ? dy : dx;
+        return __fsub_rn(__fadd_rn(b1[u], b1[v]), 1.0f);
+    }
+    const float bzx = __fadd_rn(b1[dz], b1[dx]);
+    const float bxy = __fadd_rn(b1[dx], b1[dy]);
+    const float bzy = __fadd_rn(b1[dz], b1[dy]);
+    return __fsub_rn(__fadd_rn(__fadd_rn(bzx, bxy), bzy), 5.0f);
+}
+
+}  // namespace fwi

@@ -1,0 +1,1621 @@
+// fwi3d.cu -- implementation of the C ABI declared in include/fwi3d.h.
+//
+// One translation unit: the stencil kernels (stencil.cuh), the small kernels
+// (aux_kernels.cuh) and the host runtime (context, device buffers, TMA
+// descriptors, shot batches, CUDA-graph time loops, tile autotuner).
+#include "../../include/fwi3d.h"
+
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <random>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "aux_kernels.cuh"
+#include "device.cuh"
+#include "stencil.cuh"
+
+using namespace fwi;
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Tile table (z cells = 4*TZ4, x rows = TX).  The autotuner picks one entry
+// per context and kernel; every entry is compiled for both kernels.
+// ---------------------------------------------------------------------------
+constexpr int kNumTiles = 10;
+constexpr int kTileTZ4[kNumTiles] = {16, 16, 32, 24, 25, 37, 19, 8, 32, 49};
+constexpr int kTileTX[kNumTiles] = {8, 16, 8, 8, 8, 8, 8, 16, 4, 4};
+constexpr int SHF = 7, SCF = 3;  // forward rings: halo slots, centre slots
+constexpr int SHB = 6, SCB = 2;  // backward rings
+
+template <int I>
+using TileOf = Tile<kTileTZ4[I], kTileTX[I]>;
+
+struct KInfo {
+    const void *fn = nullptr;
+    int threads = 0, tz = 0, tx = 0;
+    size_t smem = 0;
+};
+
+template <int I>
+KInfo fwd_info(bool abc)
+{
+    using T = TileOf<I>;
+    KInfo k;
+    k.threads = T::NT;
+    k.tz = T::TZ;
+    k.tx = T::TX;
+    k.smem = SHF * T::HSLOT + SCF * 2 * T::CSLOT + (SHF + SCF) * 8;
+    k.fn = abc ? (const void *)fd_forward_kernel<T, SHF, SCF, true>
+               : (const void *)fd_forward_kernel<T, SHF, SCF, false>;
+    return k;
+}
+
+template <int I>
+KInfo bwd_info(bool grad, bool dy)
+{
+    using T = TileOf<I>;
+    KInfo k;
+    k.threads = T::NT;
+    k.tz = T::TZ;
+    k.tx = T::TX;
+    k.smem = SHB * 2 * T::HSLOT + SCB * 5 * T::CSLOT + (SHB + SCB) * 8;
+    if (!grad)
+        k.fn = (const void *)fd_backward_kernel<T, SHB, SCB, false, false>;
+    else if (dy)
+        k.fn = (const void *)fd_backward_kernel<T, SHB, SCB, true, true>;
+    else
+        k.fn = (const void *)fd_backward_kernel<T, SHB, SCB, true, false>;
+    return k;
+}
+
+KInfo fwd_kernel(int tile, bool abc)
+{
+    switch (tile) {
+    case 0: return fwd_info<0>(abc);
+    case 1: return fwd_info<1>(abc);
+    case 2: return fwd_info<2>(abc);
+    case 3: return fwd_info<3>(abc);
+    case 4: return fwd_info<4>(abc);
+    case 5: return fwd_info<5>(abc);
+    case 6: return fwd_info<6>(abc);
+    case 7: return fwd_info<7>(abc);
+    case 8: return fwd_info<8>(abc);
+    default: return fwd_info<9>(abc);
+    }
+}
+
+KInfo bwd_kernel(int tile, bool grad, bool dy)
+{
+    switch (tile) {
+    case 0: return bwd_info<0>(grad, dy);
+    case 1: return bwd_info<1>(grad, dy);
+    case 2: return bwd_info<2>(grad, dy);
+    case 3: return bwd_info<3>(grad, dy);
+    case 4: return bwd_info<4>(grad, dy);
+    case 5: return bwd_info<5>(grad, dy);
+    case 6: return bwd_info<6>(grad, dy);
+    case 7: return bwd_info<7>(grad, dy);
+    case 8: return bwd_info<8>(grad, dy);
+    default: return bwd_info<9>(grad, dy);
+    }
+}
+
+// Status carried out of helpers without exceptions crossing the ABI.
+struct Fail {
+    int code;
+    std::string msg;
+};
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            throw Fail{e_ == cudaErrorMemoryAllocation ? FWI_ERR_ALLOC : FWI_ERR_CUDA,            \
+                       std::string(#call) + ": " + cudaGetErrorString(e_)};                      \
+    } while (0)
+
+[[noreturn]] void fail(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    throw Fail{code, buf};
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        CK(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !p) fail(FWI_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// 4-D map (z, x, y, shot) over a batch of pitched fields with the given box.
+CUtensorMap make_map(const float *base, int nzz, int nxx, int nyy, int ldz, int nslot, int bz, int bx)
+{
+    CUtensorMap m;
+    cuuint64_t dims[4] = {(cuuint64_t)nzz, (cuuint64_t)nxx, (cuuint64_t)nyy, (cuuint64_t)nslot};
+    cuuint64_t strides[3] = {(cuuint64_t)ldz * 4, (cuuint64_t)ldz * nxx * 4,
+                             (cuuint64_t)ldz * nxx * nyy * 4};
+    cuuint32_t box[4] = {(cuuint32_t)bz, (cuuint32_t)bx, 1, 1};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = tensor_map_encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, (void *)base, dims, strides,
+                                      box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) fail(FWI_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return m;
+}
+
+template <class T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    void ensure(size_t want)
+    {
+        if (want <= n) return;
+        release();
+        CK(cudaMalloc((void **)&p, std::max<size_t>(want, 1) * sizeof(T)));
+        n = want;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+// Grid index of a coordinate: src/modeling/modeling.cu:270-288 (FP32).
+int grid_index(float c, float dh, int nb) { return (int)((c + 0.5f * dh) / dh) + nb; }
+
+// Leapfrog stability velocity of the 8th-order 3-D operator:
+// (v dt/dh)^2 * 3 * S <= 4 with S = W0 + 2 (W1 + W2 + W3 + W4).
+double stability_velocity(double dh, double dt)
+{
+    const double S = (double)W0 + 2.0 * ((double)W1 + (double)W2 + (double)W3 + (double)W4);
+    return 2.0 / std::sqrt(3.0 * S) * dh / dt;
+}
+
+struct GraphKey {
+    int kind, n, tile, nchunk, flags;
+    bool operator<(const GraphKey &o) const
+    {
+        return std::tie(kind, n, tile, nchunk, flags) < std::tie(o.kind, o.n, o.tile, o.nchunk, o.flags);
+    }
+};
+
+struct Graph {
+    cudaGraphExec_t exec = nullptr;
+    int nodes = 0;
+    int generation = -1;
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Context
+// ---------------------------------------------------------------------------
+struct fwi_ctx {
+    fwi_grid g{};
+    fwi_params p{};
+    int nzz = 0, nxx = 0, nyy = 0, ldz = 0;
+    long long vol = 0;  // elements of one pitched field
+    float idh2 = 0, idh3 = 0;
+    int tlag = 0, nsteps = 0;
+    int B = 1;  // batch capacity
+    float vmin = 0, vmax = 0;
+    bool have_vp = false, have_geom = false;
+
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaEvent_t ev[4] = {};
+    float fwd_ms = 0, bwd_ms = 0;
+    long long launches = 0;
+    std::string err;
+
+    // device state
+    DevBuf<float> vp, vp_clean, wavelet, b1d;
+    DevBuf<float> F[2];       // forward pair [B][vol]
+    DevBuf<float> Rf[2];      // adjoint pair [B][vol]
+    DevBuf<float> acc_img, acc_ill;  // accumulators [B][vol]
+    DevBuf<float> seis_tm, data_tm, raw;
+    DevBuf<long long> rec_cell, inj_cell;
+    DevBuf<float> rec_damp;
+    DevBuf<int> inj_first, inj_rid;
+    DevBuf<BatchInfo> binfo;
+    DevBuf<double> partial, dsum;
+    DevBuf<unsigned int> ubits;
+    DevBuf<float> post;  // [nz*nx*ny] post-processing output
+    int generation = 0;  // bumped whenever a buffer a graph points at moves
+    bool acc_dirty = false;
+
+    // geometry (padded grid indices)
+    std::vector<int> sijk;  // 3 per shot
+    std::vector<int> rijk;  // 3 per receiver
+    std::vector<int> rfirst, rcount;
+    int nsrc = 0, nrec = 0;
+
+    // tuning
+    int tile_fwd = -1, tile_bwd = -1, chunk_fwd = 0, chunk_bwd = 0;
+    std::map<GraphKey, Graph> graphs;
+    std::vector<float> b1d_host;
+};
+
+namespace {
+
+void set_err(fwi_ctx *c, const Fail &f)
+{
+    if (c) c->err = f.msg;
+}
+
+template <class F>
+int guarded(fwi_ctx *c, F &&body)
+{
+    cudaGetLastError();  // a non-sticky error of an earlier call must not leak into this one
+    try {
+        body();
+        return FWI_OK;
+    } catch (const Fail &f) {
+        set_err(c, f);
+        return f.code;
+    } catch (const std::exception &e) {
+        if (c) c->err = e.what();
+        return FWI_ERR_ARG;
+    } catch (...) {
+        if (c) c->err = "unknown error";
+        return FWI_ERR_ARG;
+    }
+}
+
+int grid_blocks(long long n, int threads = 256)
+{
+    long long b = (n + threads - 1) / threads;
+    return (int)std::max(1LL, std::min(b, 148LL * 16));
+}
+
+void check_status(fwi_ctx *c)
+{
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaGetLastError());
+    unsigned int st = 0;
+    CK(cudaMemcpyFromSymbol(&st, g_status, sizeof st));
+    if (st) {
+        unsigned int z = 0;
+        CK(cudaMemcpyToSymbol(g_status, &z, sizeof z));
+        fail(FWI_ERR_TIMEOUT, "a device wait gave up (status bits 0x%x)", st);
+    }
+}
+
+// Reference wavelet (src/modeling/modeling.cu:36-59), FP32 on the host as there.
+void make_wavelet(fwi_ctx *c)
+{
+    const int nt = c->p.nt;
+    std::vector<float> w(nt);
+    const float pi = (float)M_PI;
+    float t0 = 2.0f * sqrtf(pi) / c->p.fmax;
+    float fc = c->p.fmax / (3.0f * sqrtf(pi));
+    c->tlag = (int)(t0 / c->p.dt) + 1;
+    for (int n = 0; n < nt; ++n) {
+        float td = n * c->p.dt - t0;
+        float arg = pi * pi * pi * fc * fc * td * td;
+        w[n] = 1e5f * (1.0f - 2.0f * arg) * expf(-arg);
+    }
+    c->wavelet.ensure(nt);
+    CK(cudaMemcpy(c->wavelet.p, w.data(), nt * sizeof(float), cudaMemcpyHostToDevice));
+}
+
+// Cerjan 1-D table b1d[i] = exp(-(f (nb-i))^2) (src/modeling/modeling.cu:96-99).
+void make_b1d(fwi_ctx *c)
+{
+    const int nb = c->g.nb;
+    c->b1d_host.assign(nb, 1.0f);
+    for (int i = 0; i < nb; ++i) c->b1d_host[i] = expf(-powf(c->p.abc_factor * (nb - i), 2.0f));
+    c->b1d.ensure(nb);
+    CK(cudaMemcpy(c->b1d.p, c->b1d_host.data(), nb * sizeof(float), cudaMemcpyHostToDevice));
+}
+
+// Host copy of the Cerjan factor (for receiver samples).
+float host_cerjan(const fwi_ctx *c, int i, int j, int k)
+{
+    auto depth = [&](int x, int n) { return x < c->g.nb ? x : (x >= n - c->g.nb ? n - 1 - x : -1); };
+    const float *b1 = c->b1d_host.data();
+    int dz = depth(i, c->nzz), dx = depth(j, c->nxx), dy = depth(k, c->nyy);
+    int n = (dz >= 0) + (dx >= 0) + (dy >= 0);
+    if (n == 0) return 1.0f;
+    if (n == 1) return b1[dz >= 0 ? dz : (dx >= 0 ? dx : dy)];
+    if (n == 2) {
+        int u = dz >= 0 ? dz : dx, v = dy >= 0 ? dy : dx;
+        volatile float s = b1[u] + b1[v];
+        return s - 1.0f;
+    }
+    volatile float bzx = b1[dz] + b1[dx], bxy = b1[dx] + b1[dy], bzy = b1[dz] + b1[dy];
+    volatile float s = bzx + bxy;
+    volatile float s2 = s + bzy;
+    return s2 - 5.0f;
+}
+
+void ensure_fields(fwi_ctx *c, bool adjoint)
+{
+    const size_t n = (size_t)c->B * c->vol;
+    bool moved = false;
+    for (int k = 0; k < 2; ++k) {
+        if (c->F[k].n < n) moved = true;
+        c->F[k].ensure(n);
+    }
+    if (adjoint) {
+        for (int k = 0; k < 2; ++k) {
+            if (c->Rf[k].n < n) moved = true;
+            c->Rf[k].ensure(n);
+        }
+        if (c->acc_img.n < n) {
+            moved = true;
+            c->acc_img.ensure(n);
+            c->acc_ill.ensure(n);
+            CK(cudaMemsetAsync(c->acc_img.p, 0, n * sizeof(float), c->stream));
+            CK(cudaMemsetAsync(c->acc_ill.p, 0, n * sizeof(float), c->stream));
+        }
+    }
+    if (moved) ++c->generation;
+}
+
+// Per-batch shot tables: sources, receivers (flat cells, damping) and the
+// distinct receiver cells with their receivers (injection lists).
+struct BatchTables {
+    BatchInfo info{};
+    std::vector<long long> cell;
+    std::vector<float> damp;
+    std::vector<long long> ucell;
+    std::vector<int> ufirst, urid;
+    std::vector<int> shot_nrec;
+};
+
+BatchTables build_batch(fwi_ctx *c, const int *shots, int n)
+{
+    BatchTables t;
+    t.info.nshot = n;
+    const bool abc = c->p.boundary == FWI_BOUNDARY_ABC;
+    for (int s = 0; s < n; ++s) {
+        const int id = shots[s];
+        if (id < 0 || id >= c->nsrc) fail(FWI_ERR_ARG, "shot %d out of range [0,%d)", id, c->nsrc);
+        for (int a = 0; a < 3; ++a) t.info.src[s][a] = c->sijk[3 * id + a];
+        const int f = c->rfirst[id], m = c->rcount[id];
+        t.shot_nrec.push_back(m);
+        for (int r = f; r < f + m; ++r) {
+            const int i = c->rijk[3 * r], j = c->rijk[3 * r + 1], k = c->rijk[3 * r + 2];
+            t.cell.push_back((long long)s * c->vol + i + (long long)j * c->ldz + (long long)k * c->ldz * c->nxx);
+            t.damp.push_back(abc ? host_cerjan(c, i, j, k) : 1.0f);
+        }
+    }
+    t.info.R = (int)t.cell.size();
+    std::vector<int> order(t.info.R);
+    for (int r = 0; r < t.info.R; ++r) order[r] = r;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return t.cell[a] < t.cell[b]; });
+    for (int q = 0; q < t.info.R; ++q) {
+        const int r = order[q];
+        if (t.ucell.empty() || t.ucell.back() != t.cell[r]) {
+            t.ucell.push_back(t.cell[r]);
+            t.ufirst.push_back(q);
+        }
+        t.urid.push_back(r);
+    }
+    t.ufirst.push_back(t.info.R);
+    t.info.ncell = (int)t.ucell.size();
+    return t;
+}
+
+void upload_batch(fwi_ctx *c, const BatchTables &t)
+{
+    const int R = std::max(t.info.R, 1);
+    if (c->rec_cell.n < (size_t)R || c->inj_first.n < (size_t)R + 1) {
+        c->rec_cell.ensure(R);
+        c->rec_damp.ensure(R);
+        c->inj_cell.ensure(R);
+        c->inj_first.ensure(R + 1);
+        c->inj_rid.ensure(R);
+        ++c->generation;
+    }
+    const size_t need = (size_t)c->p.nt * R;
+    if (c->seis_tm.n < need || c->data_tm.n < need || c->raw.n < need) {
+        c->seis_tm.ensure(need);
+        c->data_tm.ensure(need);
+        c->raw.ensure(need);
+        ++c->generation;
+    }
+    c->binfo.ensure(1);
+    CK(cudaMemcpyAsync(c->binfo.p, &t.info, sizeof(BatchInfo), cudaMemcpyHostToDevice, c->stream));
+    if (t.info.R) {
+        CK(cudaMemcpyAsync(c->rec_cell.p, t.cell.data(), t.info.R * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->rec_damp.p, t.damp.data(), t.info.R * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->inj_cell.p, t.ucell.data(), t.ucell.size() * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->inj_first.p, t.ufirst.data(), t.ufirst.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->inj_rid.p, t.urid.data(), t.urid.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    }
+    // the host vectors die with t: make the copies complete before returning
+    CK(cudaStreamSynchronize(c->stream));
+}
+
+// Number of z tiles, x tiles and the y chunk length for a tile / chunk count.
+void tiling(const fwi_ctx *c, const KInfo &k, int nchunk, int &ntz, int &ntx, int &ylen)
+{
+    ntz = (c->nzz - 8 + k.tz - 1) / k.tz;
+    ntx = (c->nxx - 8 + k.tx - 1) / k.tx;
+    ylen = (c->nyy - 8 + nchunk - 1) / nchunk;
+}
+
+void prepare_kernel(const KInfo &k)
+{
+    CK(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem));
+}
+
+// Chunks along y so that the grid fills the GPU about twice per resident wave.
+int default_chunks(const fwi_ctx *c, const KInfo &k, int nshot)
+{
+    prepare_kernel(k);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, k.threads, k.smem);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    per_sm = std::max(per_sm, 1);
+    int ntz, ntx, ylen;
+    tiling(c, k, 1, ntz, ntx, ylen);
+    const long long cols = (long long)ntz * ntx * nshot;
+    const long long slots = (long long)per_sm * sms;
+    int nchunk = (int)std::max(1LL, (slots + cols - 1) / cols);
+    // keep at least ~24 planes per chunk so the 8-plane warm-up stays small
+    nchunk = std::min(nchunk, std::max(1, (c->nyy - 8) / 24));
+    return nchunk;
+}
+
+// Heuristic tile before tuning: least wasted z cells, then least x waste.
+int default_tile(const fwi_ctx *c, bool backward)
+{
+    int best = 0;
+    double best_cost = 1e30;
+    for (int t = 0; t < kNumTiles; ++t) {
+        const int tz = 4 * kTileTZ4[t], tx = kTileTX[t];
+        const int nzi = c->nzz - 8, nxi = c->nxx - 8;
+        const double wz = (double)((nzi + tz - 1) / tz * tz) / nzi;
+        const double wx = (double)((nxi + tx - 1) / tx * tx) / nxi;
+        const double halo = (double)(tz + 8) * (tx + 8) / (tz * tx);
+        const double cost = wz * wx * (1.0 + (backward ? 0.30 : 0.15) * halo);
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = t;
+        }
+    }
+    return best;
+}
+
+// ---------------------------------------------------------------------------
+// Launch builders
+// ---------------------------------------------------------------------------
+struct FwdLaunch {
+    KInfo k;
+    dim3 grid;
+    CUtensorMap mh[2], mq[2], mv;
+    FwdArgs a;
+};
+
+FwdLaunch make_fwd(fwi_ctx *c, int n, int tile, int nchunk, bool record)
+{
+    FwdLaunch L;
+    const bool abc = c->p.boundary == FWI_BOUNDARY_ABC;
+    L.k = fwd_kernel(tile, abc);
+    prepare_kernel(L.k);
+    int ntz, ntx, ylen;
+    tiling(c, L.k, nchunk, ntz, ntx, ylen);
+    L.grid = dim3(ntz * ntx * nchunk, n, 1);
+    for (int b = 0; b < 2; ++b) {
+        L.mh[b] = make_map(c->F[b].p, c->nzz, c->nxx, c->nyy, c->ldz, n, L.k.tz + 8, L.k.tx + 8);
+        L.mq[b] = make_map(c->F[b].p, c->nzz, c->nxx, c->nyy, c->ldz, n, L.k.tz, L.k.tx);
+    }
+    L.mv = make_map(c->vp.p, c->nzz, c->nxx, c->nyy, c->ldz, 1, L.k.tz, L.k.tx);
+    FwdArgs &a = L.a;
+    memset(&a, 0, sizeof a);
+    a.nzz = c->nzz;
+    a.nxx = c->nxx;
+    a.nyy = c->nyy;
+    a.ldz = c->ldz;
+    a.vol = c->vol;
+    a.ntz = ntz;
+    a.ntx = ntx;
+    a.ylen = ylen;
+    a.nt = c->p.nt;
+    a.tlag = record ? c->tlag : (1 << 30);
+    a.cvel = c->p.dt * c->p.dt * c->idh2;
+    a.idh3 = c->idh3;
+    a.nb = c->g.nb;
+    a.b1d = abc ? c->b1d.p : nullptr;
+    a.wavelet = c->wavelet.p;
+    a.binfo = c->binfo.p;
+    a.rec_cell = c->rec_cell.p;
+    a.rec_damp = c->rec_damp.p;
+    a.seis_tm = c->seis_tm.p;
+    return L;
+}
+
+void launch_fwd(fwi_ctx *c, FwdLaunch &L, int t, int cur)
+{
+    FwdArgs a = L.a;
+    a.t = t;
+    a.A = c->F[cur].p;
+    a.Q = c->F[1 - cur].p;
+    void *args[] = {&L.mh[cur], &L.mq[1 - cur], &L.mv, &a};
+    CK(cudaLaunchKernel(L.k.fn, L.grid, dim3(L.k.threads), args, L.k.smem, c->stream));
+}
+
+struct BwdLaunch {
+    KInfo k;
+    dim3 grid;
+    CUtensorMap mhs[2], mhr[2], mcs[2], mcr[2], mv, mim, mil;
+    BwdArgs a;
+};
+
+BwdLaunch make_bwd(fwi_ctx *c, int n, int tile, int nchunk, bool grad)
+{
+    BwdLaunch L;
+    L.k = bwd_kernel(tile, grad, (c->p.flags & FWI_FLAG_GRAD_DY) != 0);
+    prepare_kernel(L.k);
+    int ntz, ntx, ylen;
+    tiling(c, L.k, nchunk, ntz, ntx, ylen);
+    L.grid = dim3(ntz * ntx * nchunk, n, 1);
+    for (int b = 0; b < 2; ++b) {
+        L.mhs[b] = make_map(c->F[b].p, c->nzz, c->nxx, c->nyy, c->ldz, n, L.k.tz + 8, L.k.tx + 8);
+        L.mhr[b] = make_map(c->Rf[b].p, c->nzz, c->nxx, c->nyy, c->ldz, n, L.k.tz + 8, L.k.tx + 8);
+        L.mcs[b] = make_map(c->F[b].p, c->nzz, c->nxx, c->nyy, c->ldz, n, L.k.tz, L.k.tx);
+        L.mcr[b] = make_map(c->Rf[b].p, c->nzz, c->nxx, c->nyy, c->ldz, n, L.k.tz, L.k.tx);
+    }
+    L.mv = make_map(c->vp.p, c->nzz, c->nxx, c->nyy, c->ldz, 1, L.k.tz, L.k.tx);
+    L.mim = make_map(c->acc_img.p, c->nzz, c->nxx, c->nyy, c->ldz, n, L.k.tz, L.k.tx);
+    L.mil = make_map(c->acc_ill.p, c->nzz, c->nxx, c->nyy, c->ldz, n, L.k.tz, L.k.tx);
+    BwdArgs &a = L.a;
+    memset(&a, 0, sizeof a);
+    a.nzz = c->nzz;
+    a.nxx = c->nxx;
+    a.nyy = c->nyy;
+    a.ldz = c->ldz;
+    a.vol = c->vol;
+    a.ntz = ntz;
+    a.ntx = ntx;
+    a.ylen = ylen;
+    a.nt = c->p.nt;
+    a.nsteps = c->nsteps;
+    a.cvel = c->p.dt * c->p.dt * c->idh2;
+    a.gscale = c->p.dt * c->idh2;
+    a.idh3 = c->idh3;
+    a.subtract_src = (c->p.flags & FWI_FLAG_SUBTRACT_SOURCE) ? 1 : 0;
+    a.image = c->acc_img.p;
+    a.illum = c->acc_ill.p;
+    a.wavelet = c->wavelet.p;
+    a.binfo = c->binfo.p;
+    return L;
+}
+
+void launch_bwd(fwi_ctx *c, BwdLaunch &L, int t, int scur, int rcur)
+{
+    BwdArgs a = L.a;
+    a.t = t;
+    a.Psold = c->F[scur].p;
+    a.Ps = c->F[1 - scur].p;
+    a.Pr = c->Rf[rcur].p;
+    a.Prold = c->Rf[1 - rcur].p;
+    void *args[] = {&L.mhs[scur], &L.mhr[rcur], &L.mcs[1 - scur], &L.mcr[1 - rcur],
+                    &L.mv,        &L.mim,       &L.mil,          &a};
+    CK(cudaLaunchKernel(L.k.fn, L.grid, dim3(L.k.threads), args, L.k.smem, c->stream));
+}
+
+void launch_inject(fwi_ctx *c, int t, int rcur)
+{
+    const int sample = c->p.nt - 1 - t;
+    inject_adjoint_kernel<<<64, 256, 0, c->stream>>>(c->Rf[rcur].p, c->binfo.p, c->inj_cell.p,
+                                                     c->inj_first.p, c->inj_rid.p, c->data_tm.p,
+                                                     sample, c->idh3);
+    CK(cudaGetLastError());
+}
+
+int tuned_fwd(fwi_ctx *c) { return c->tile_fwd >= 0 ? c->tile_fwd : default_tile(c, false); }
+int tuned_bwd(fwi_ctx *c) { return c->tile_bwd >= 0 ? c->tile_bwd : default_tile(c, true); }
+
+// ---------------------------------------------------------------------------
+// Time loops, captured once per (kind, batch size, tiles) as CUDA graphs.
+// kind 0: forward with receivers, 1: forward without, 2: backward image,
+// 3: backward gradient.  The fields start from the state the caller left.
+// ---------------------------------------------------------------------------
+Graph &time_loop_graph(fwi_ctx *c, int kind, int n)
+{
+    const int tile = kind < 2 ? tuned_fwd(c) : tuned_bwd(c);
+    int nchunk = kind < 2 ? c->chunk_fwd : c->chunk_bwd;
+    if (nchunk <= 0)
+        nchunk = kind < 2 ? default_chunks(c, fwd_kernel(tile, c->p.boundary == FWI_BOUNDARY_ABC), n)
+                          : default_chunks(c, bwd_kernel(tile, kind == 3, false), n);
+    GraphKey key{kind, n, tile, nchunk, c->p.flags};
+    Graph &gr = c->graphs[key];
+    if (gr.exec && gr.generation == c->generation) return gr;
+    if (gr.exec) {
+        cudaGraphExecDestroy(gr.exec);
+        gr.exec = nullptr;
+    }
+    const int N = c->nsteps;
+    // descriptors, kernel attributes and occupancy queries before capture
+    FwdLaunch LF;
+    BwdLaunch LB;
+    if (kind < 2)
+        LF = make_fwd(c, n, tile, nchunk, kind == 0);
+    else
+        LB = make_bwd(c, n, tile, nchunk, kind == 3);
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+        int nodes = 0;
+        if (kind < 2) {
+            CK(cudaEventRecordWithFlags(c->ev[0], c->stream, cudaEventRecordExternal));
+            for (int t = 0; t < N; ++t) {
+                launch_fwd(c, LF, t, t & 1);
+                ++nodes;
+            }
+            CK(cudaEventRecordWithFlags(c->ev[1], c->stream, cudaEventRecordExternal));
+        } else {
+            // the forward pass leaves u^N in F[N%2] and u^{N-1} in F[1-N%2]
+            const int s0 = 1 - (N & 1);
+            CK(cudaEventRecordWithFlags(c->ev[2], c->stream, cudaEventRecordExternal));
+            for (int t = 0; t < N; ++t) {
+                const int scur = (s0 + t) & 1, rcur = t & 1;
+                if (t < c->p.nt) {
+                    launch_inject(c, t, rcur);
+                    ++nodes;
+                }
+                launch_bwd(c, LB, t, scur, rcur);
+                ++nodes;
+            }
+            CK(cudaEventRecordWithFlags(c->ev[3], c->stream, cudaEventRecordExternal));
+        }
+        gr.nodes = nodes;
+    } catch (...) {
+        cudaStreamEndCapture(c->stream, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        throw;
+    }
+    CK(cudaStreamEndCapture(c->stream, &graph));
+    cudaError_t e = cudaGraphInstantiate(&gr.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) fail(FWI_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    gr.generation = c->generation;
+    return gr;
+}
+
+void run_graph(fwi_ctx *c, Graph &g)
+{
+    CK(cudaGraphLaunch(g.exec, c->stream));
+    c->launches += g.nodes;
+}
+
+// Zero both forward fields of the batch and add source sample 0.
+void start_forward(fwi_ctx *c, int n)
+{
+    const size_t bytes = (size_t)n * c->vol * sizeof(float);
+    CK(cudaMemsetAsync(c->F[0].p, 0, bytes, c->stream));
+    CK(cudaMemsetAsync(c->F[1].p, 0, bytes, c->stream));
+    if (c->p.nt > 0) {
+        start_source_kernel<<<1, kMaxBatch, 0, c->stream>>>(c->F[0].p, c->vol, c->ldz, c->nxx, c->binfo.p,
+                                                            c->wavelet.p, c->idh3);
+        CK(cudaGetLastError());
+        ++c->launches;
+    }
+}
+
+void require_ready(fwi_ctx *c)
+{
+    if (!c->have_vp) fail(FWI_ERR_STATE, "no velocity model set");
+    if (!c->have_geom) fail(FWI_ERR_STATE, "no geometry set");
+}
+
+// Device seismogram block [nt][R] -> Fortran per shot [R][nt] at dst.
+void seis_to_fortran(fwi_ctx *c, int R, float *dst)
+{
+    dim3 grid((R + 31) / 32, (c->p.nt + 31) / 32);
+    transpose_kernel<<<grid, dim3(32, 8), 0, c->stream>>>(c->seis_tm.p, c->p.nt, R, dst);
+    CK(cudaGetLastError());
+    ++c->launches;
+}
+
+// Fortran per shot [R][nt] at src (device) -> data_tm [nt][R].
+void data_from_fortran(fwi_ctx *c, int R, const float *src)
+{
+    dim3 grid((c->p.nt + 31) / 32, (R + 31) / 32);
+    transpose_kernel<<<grid, dim3(32, 8), 0, c->stream>>>(src, R, c->p.nt, c->data_tm.p);
+    CK(cudaGetLastError());
+    ++c->launches;
+}
+
+// Forward modeling of a list of shots in batches of B.
+void model_impl(fwi_ctx *c, const int *shots, int nshots, float *out, bool out_is_device)
+{
+    require_ready(c);
+    ensure_fields(c, false);
+    float total_ms = 0;
+    size_t off = 0;
+    for (int s0 = 0; s0 < nshots; s0 += c->B) {
+        const int n = std::min(c->B, nshots - s0);
+        BatchTables t = build_batch(c, shots + s0, n);
+        upload_batch(c, t);
+        const int R = t.info.R;
+        if (R) CK(cudaMemsetAsync(c->seis_tm.p, 0, (size_t)c->p.nt * R * sizeof(float), c->stream));
+        start_forward(c, n);
+        Graph &g = time_loop_graph(c, 0, c->B);
+        run_graph(c, g);
+        const size_t cnt = (size_t)c->p.nt * R;
+        if (R) {
+            if (out_is_device) {
+                seis_to_fortran(c, R, out + off);
+            } else {
+                seis_to_fortran(c, R, c->raw.p);
+                CK(cudaMemcpyAsync(out + off, c->raw.p, cnt * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+            }
+        }
+        check_status(c);
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+        total_ms += ms;
+        off += cnt;
+    }
+    c->fwd_ms = total_ms;
+    c->bwd_ms = 0;
+}
+
+// Forward (no receivers) + fused backward of a list of shots.
+void migrate_impl(fwi_ctx *c, const int *shots, int nshots, const float *data, bool data_is_device,
+                  bool grad)
+{
+    require_ready(c);
+    if (c->p.boundary == FWI_BOUNDARY_ABC)
+        fail(FWI_ERR_STATE, "back-propagation needs a non-damping (random) boundary context");
+    ensure_fields(c, true);
+    float f_ms = 0, b_ms = 0;
+    size_t off = 0;
+    for (int s0 = 0; s0 < nshots; s0 += c->B) {
+        const int n = std::min(c->B, nshots - s0);
+        BatchTables t = build_batch(c, shots + s0, n);
+        upload_batch(c, t);
+        const int R = t.info.R;
+        const size_t cnt = (size_t)c->p.nt * R;
+        if (R) {
+            if (data_is_device) {
+                data_from_fortran(c, R, data + off);
+            } else {
+                CK(cudaMemcpyAsync(c->raw.p, data + off, cnt * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+                data_from_fortran(c, R, c->raw.p);
+            }
+        }
+        start_forward(c, n);
+        Graph &gf = time_loop_graph(c, 1, c->B);
+        run_graph(c, gf);
+        const size_t bytes = (size_t)n * c->vol * sizeof(float);
+        CK(cudaMemsetAsync(c->Rf[0].p, 0, bytes, c->stream));
+        CK(cudaMemsetAsync(c->Rf[1].p, 0, bytes, c->stream));
+        Graph &gb = time_loop_graph(c, grad ? 3 : 2, c->B);
+        run_graph(c, gb);
+        check_status(c);
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+        f_ms += ms;
+        CK(cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]));
+        b_ms += ms;
+        off += cnt;
+        c->acc_dirty = true;
+    }
+    c->fwd_ms = f_ms;
+    c->bwd_ms = b_ms;
+}
+
+// Fold the per-slot accumulators into slot 0.
+void fold_accumulators(fwi_ctx *c)
+{
+    if (!c->acc_img.p) fail(FWI_ERR_STATE, "no image or gradient has been accumulated");
+    if (c->B > 1 && c->acc_dirty) {
+        sum_slots_kernel<<<grid_blocks(c->vol), 256, 0, c->stream>>>(c->acc_img.p, c->vol, c->B);
+        sum_slots_kernel<<<grid_blocks(c->vol), 256, 0, c->stream>>>(c->acc_ill.p, c->vol, c->B);
+        CK(cudaGetLastError());
+        c->launches += 2;
+    }
+    c->acc_dirty = false;
+}
+
+// FP64 sum of squares of obs-cal (and the residual) with fixed-order partials.
+constexpr int kRedThreads = 256, kRedBlocks = 296;
+
+double residual_impl(fwi_ctx *c, const float *d_obs, const float *d_cal, long long n, float *d_res)
+{
+    c->partial.ensure(kRedBlocks);
+    c->dsum.ensure(1);
+    residual_partial_kernel<kRedThreads><<<kRedBlocks, kRedThreads, 0, c->stream>>>(d_obs, d_cal, n, d_res,
+                                                                                   c->partial.p);
+    finish_sum_kernel<kRedThreads><<<1, kRedThreads, 0, c->stream>>>(c->partial.p, kRedBlocks, c->dsum.p);
+    CK(cudaGetLastError());
+    c->launches += 2;
+    double s = 0;
+    CK(cudaMemcpyAsync(&s, c->dsum.p, sizeof s, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return s;
+}
+
+// Host Poisson-disk sampling in a box (Bridson's method, as
+// poissonDiskSampling of src/admin/admin.cpp:138-241: 30 candidates in the
+// shell [r, 2r] around a random active point), seeded and deterministic.
+std::vector<float> poisson_points(float xm, float ym, float zm, float r, std::mt19937_64 &rng)
+{
+    const float cell = r / std::sqrt(3.0f);
+    const int gx = std::max(1, (int)std::ceil(xm / cell)), gy = std::max(1, (int)std::ceil(ym / cell)),
+              gz = std::max(1, (int)std::ceil(zm / cell));
+    std::vector<int> grid((size_t)gx * gy * gz, -1);
+    std::vector<float> pts;  // x, y, z triples
+    std::vector<int> active;
+    std::uniform_real_distribution<float> U(0.0f, 1.0f);
+    auto cell_of = [&](float x, float y, float z, int &a, int &b, int &d) {
+        a = std::min(gx - 1, (int)(x / cell));
+        b = std::min(gy - 1, (int)(y / cell));
+        d = std::min(gz - 1, (int)(z / cell));
+    };
+    auto insert = [&](float x, float y, float z) {
+        int a, b, d;
+        cell_of(x, y, z, a, b, d);
+        grid[d + (size_t)gz * (a + (size_t)gx * b)] = (int)(pts.size() / 3);
+        pts.push_back(x);
+        pts.push_back(y);
+        pts.push_back(z);
+        active.push_back((int)(pts.size() / 3) - 1);
+    };
+    auto valid = [&](float x, float y, float z) {
+        if (x < 0 || y < 0 || z < 0 || x >= xm || y >= ym || z >= zm) return false;
+        int a, b, d;
+        cell_of(x, y, z, a, b, d);
+        for (int k = -2; k <= 2; ++k)
+            for (int j = -2; j <= 2; ++j)
+                for (int i = -2; i <= 2; ++i) {
+                    const int A = a + j, Bq = b + k, D = d + i;
+                    if (A < 0 || Bq < 0 || D < 0 || A >= gx || Bq >= gy || D >= gz) continue;
+                    const int q = grid[D + (size_t)gz * (A + (size_t)gx * Bq)];
+                    if (q < 0) continue;
+                    const float dx = pts[3 * q] - x, dy = pts[3 * q + 1] - y, dz = pts[3 * q + 2] - z;
+                    if (dx * dx + dy * dy + dz * dz < r * r) return false;
+                }
+        return true;
+    };
+    insert(U(rng) * xm, U(rng) * ym, U(rng) * zm);
+    const float pi = (float)M_PI;
+    while (!active.empty()) {
+        const int ai = (int)(U(rng) * active.size()) % (int)active.size();
+        const int q = active[ai];
+        bool found = false;
+        for (int tries = 0; tries < 30; ++tries) {
+            const float th = 2.0f * pi * U(rng), ph = pi * U(rng), rr = r * (1.0f + U(rng));
+            const float x = pts[3 * q] + rr * sinf(ph) * cosf(th);
+            const float y = pts[3 * q + 1] + rr * sinf(ph) * sinf(th);
+            const float z = pts[3 * q + 2] + rr * cosf(ph);
+            if (valid(x, y, z)) {
+                insert(x, y, z);
+                found = true;
+            }
+        }
+        if (!found) {
+            active[ai] = active.back();
+            active.pop_back();
+        }
+    }
+    return pts;
+}
+
+float device_max_abs(fwi_ctx *c, const float *v)
+{
+    c->ubits.ensure(1);
+    CK(cudaMemsetAsync(c->ubits.p, 0, sizeof(unsigned), c->stream));
+    max_abs_kernel<<<grid_blocks(c->vol), 256, 0, c->stream>>>(v, c->vol, c->ldz, c->nzz, c->ubits.p);
+    CK(cudaGetLastError());
+    unsigned bits = 0;
+    CK(cudaMemcpyAsync(&bits, c->ubits.p, sizeof bits, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    float f;
+    memcpy(&f, &bits, sizeof f);
+    return f;
+}
+
+void check_cfl(fwi_ctx *c)
+{
+    const float vm = device_max_abs(c, c->vp.p);
+    const double lim = stability_velocity(c->g.dh, c->p.dt);
+    if (!(vm <= lim))
+        fail(FWI_ERR_NUMERIC, "velocity %.1f m/s exceeds the leapfrog stability limit %.1f m/s (dh=%g, dt=%g)",
+             vm, lim, c->g.dh, c->p.dt);
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char *fwi_status_string(int s)
+{
+    switch (s) {
+    case FWI_OK: return "ok";
+    case FWI_ERR_ARG: return "invalid argument";
+    case FWI_ERR_CUDA: return "CUDA error";
+    case FWI_ERR_ALLOC: return "device allocation failed";
+    case FWI_ERR_TIMEOUT: return "device wait timed out";
+    case FWI_ERR_STATE: return "call out of order";
+    case FWI_ERR_IO: return "file could not be opened";
+    case FWI_ERR_NUMERIC: return "numerical check failed";
+    case FWI_ERR_NODEV: return "no CUDA device";
+    default: return "unknown status";
+    }
+}
+
+int fwi_last_error(fwi_ctx *c, char *buf, int n)
+{
+    if (!c || !buf || n <= 0) return FWI_ERR_ARG;
+    snprintf(buf, n, "%s", c->err.c_str());
+    return FWI_OK;
+}
+
+int fwi_num_tiles(int *n)
+{
+    if (!n) return FWI_ERR_ARG;
+    *n = kNumTiles;
+    return FWI_OK;
+}
+
+int fwi_tile_shape(int tile, int *tz, int *tx)
+{
+    if (tile < 0 || tile >= kNumTiles || !tz || !tx) return FWI_ERR_ARG;
+    *tz = 4 * kTileTZ4[tile];
+    *tx = kTileTX[tile];
+    return FWI_OK;
+}
+
+int fwi_create(const fwi_grid *grid, const fwi_params *params, fwi_ctx **out)
+{
+    if (!grid || !params || !out) return FWI_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return FWI_ERR_NODEV;
+    }
+    fwi_ctx *c = new fwi_ctx();
+    int st = guarded(c, [&] {
+        c->g = *grid;
+        c->p = *params;
+        if (grid->nz < 1 || grid->nx < 1 || grid->ny < 1) fail(FWI_ERR_ARG, "empty model");
+        if (grid->nb < 4) fail(FWI_ERR_ARG, "pad width nb=%d < 4 (the stencil needs 4 cells)", grid->nb);
+        if (grid->nb > kMaxPad) fail(FWI_ERR_ARG, "pad width nb=%d > %d", grid->nb, kMaxPad);
+        if (!(grid->dh > 0) || !(params->dt > 0) || !(params->fmax > 0) || params->nt < 1)
+            fail(FWI_ERR_ARG, "dh, dt, fmax and nt must be positive");
+        if (params->boundary != FWI_BOUNDARY_ABC && params->boundary != FWI_BOUNDARY_RBC)
+            fail(FWI_ERR_ARG, "unknown boundary kind %d", params->boundary);
+        c->B = std::max(1, std::min(params->max_batch, kMaxBatch));
+        c->nzz = grid->nz + 2 * grid->nb;
+        c->nxx = grid->nx + 2 * grid->nb;
+        c->nyy = grid->ny + 2 * grid->nb;
+        c->ldz = (c->nzz + 7) / 8 * 8;
+        c->vol = (long long)c->ldz * c->nxx * c->nyy;
+        c->idh2 = 1.0f / (grid->dh * grid->dh);
+        c->idh3 = 1.0f / (grid->dh * grid->dh * grid->dh);
+        CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->own_stream = true;
+        for (auto &e : c->ev) CK(cudaEventCreate(&e));
+        make_wavelet(c);
+        c->nsteps = c->tlag + c->p.nt;
+        make_b1d(c);
+        c->vp.ensure(c->vol);
+        c->vp_clean.ensure(c->vol);
+        CK(cudaMemset(c->vp.p, 0, c->vol * sizeof(float)));
+        c->binfo.ensure(1);
+        BatchInfo z{};
+        CK(cudaMemcpy(c->binfo.p, &z, sizeof z, cudaMemcpyHostToDevice));
+    });
+    if (st != FWI_OK) {
+        fprintf(stderr, "fwi_create: %s\n", c->err.c_str());
+        fwi_destroy(c);
+        return st;
+    }
+    *out = c;
+    return FWI_OK;
+}
+
+int fwi_destroy(fwi_ctx *c)
+{
+    if (!c) return FWI_ERR_ARG;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto &kv : c->graphs)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    c->vp.release();
+    c->vp_clean.release();
+    c->wavelet.release();
+    c->b1d.release();
+    for (auto &f : c->F) f.release();
+    for (auto &f : c->Rf) f.release();
+    c->acc_img.release();
+    c->acc_ill.release();
+    c->seis_tm.release();
+    c->data_tm.release();
+    c->raw.release();
+    c->rec_cell.release();
+    c->rec_damp.release();
+    c->inj_cell.release();
+    c->inj_first.release();
+    c->inj_rid.release();
+    c->binfo.release();
+    c->partial.release();
+    c->dsum.release();
+    c->ubits.release();
+    c->post.release();
+    for (auto &e : c->ev)
+        if (e) cudaEventDestroy(e);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return FWI_OK;
+}
+
+int fwi_set_stream(fwi_ctx *c, void *stream)
+{
+    if (!c) return FWI_ERR_ARG;
+    return guarded(c, [&] {
+        CK(cudaStreamSynchronize(c->stream));
+        if (c->own_stream) CK(cudaStreamDestroy(c->stream));
+        c->own_stream = false;
+        c->stream = (cudaStream_t)stream;
+    });
+}
+
+int fwi_get_dims(fwi_ctx *c, int *nzz, int *nxx, int *nyy, int *ldz, int *tlag)
+{
+    if (!c) return FWI_ERR_ARG;
+    if (nzz) *nzz = c->nzz;
+    if (nxx) *nxx = c->nxx;
+    if (nyy) *nyy = c->nyy;
+    if (ldz) *ldz = c->ldz;
+    if (tlag) *tlag = c->tlag;
+    return FWI_OK;
+}
+
+int fwi_set_velocity(fwi_ctx *c, const float *vp)
+{
+    if (!c || !vp) return FWI_ERR_ARG;
+    return guarded(c, [&] {
+        const size_t n = (size_t)c->g.nz * c->g.nx * c->g.ny;
+        float lo = 1e30f, hi = -1e30f;
+        for (size_t i = 0; i < n; ++i) {
+            if (!std::isfinite(vp[i]) || vp[i] <= 0) fail(FWI_ERR_NUMERIC, "velocity[%zu] = %g is not a positive number", i, vp[i]);
+            lo = std::min(lo, vp[i]);
+            hi = std::max(hi, vp[i]);
+        }
+        c->vmin = lo;
+        c->vmax = hi;
+        float *d_in = nullptr;
+        CK(cudaMalloc((void **)&d_in, n * sizeof(float)));
+        cudaError_t e = cudaMemcpyAsync(d_in, vp, n * sizeof(float), cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess) {
+            pad_edges_kernel<<<grid_blocks(c->vol), 256, 0, c->stream>>>(d_in, c->g.nz, c->g.nx, c->g.ny, c->g.nb,
+                                                                         c->nzz, c->nxx, c->nyy, c->ldz, c->vp.p);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(c->vp_clean.p, c->vp.p, c->vol * sizeof(float), cudaMemcpyDeviceToDevice, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        cudaFree(d_in);
+        CK(e);
+        c->launches += 1;
+        check_cfl(c);
+        c->have_vp = true;
+    });
+}
+
+int fwi_set_padded_velocity(fwi_ctx *c, const float *vpp)
+{
+    if (!c || !vpp) return FWI_ERR_ARG;
+    return guarded(c, [&] {
+        const size_t n = (size_t)c->nzz * c->nxx * c->nyy;
+        float lo = 1e30f, hi = -1e30f;
+        for (size_t i = 0; i < n; ++i) {
+            if (!std::isfinite(vpp[i]) || vpp[i] <= 0) fail(FWI_ERR_NUMERIC, "velocity[%zu] = %g is not a positive number", i, vpp[i]);
+            lo = std::min(lo, vpp[i]);
+            hi = std::max(hi, vpp[i]);
+        }
+        c->vmin = lo;
+        c->vmax = hi;
+        float *d_in = nullptr;
+        CK(cudaMalloc((void **)&d_in, n * sizeof(float)));
+        cudaError_t e = cudaMemcpyAsync(d_in, vpp, n * sizeof(float), cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess) {
+            dense_to_pitched_kernel<<<grid_blocks(c->vol), 256, 0, c->stream>>>(d_in, c->nzz, c->nxx, c->nyy, c->ldz,
+                                                                                c->vp.p);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(c->vp_clean.p, c->vp.p, c->vol * sizeof(float), cudaMemcpyDeviceToDevice, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        cudaFree(d_in);
+        CK(e);
+        c->launches += 1;
+        check_cfl(c);
+        c->have_vp = true;
+    });
+}
+
+int fwi_get_padded_velocity(fwi_ctx *c, float *vpp)
+{
+    if (!c || !vpp) return FWI_ERR_ARG;
+    return guarded(c, [&] {
+        const size_t n = (size_t)c->nzz * c->nxx * c->nyy;
+        float *d_out = nullptr;
+        CK(cudaMalloc((void **)&d_out, n * sizeof(float)));
+        pitched_to_dense_kernel<<<grid_blocks(n), 256, 0, c->stream>>>(c->vp.p, c->nzz, c->nxx, c->nyy, c->ldz, d_out);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(vpp, d_out, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        cudaFree(d_out);
+        CK(e);
+        c->launches += 1;
+    });
+}
+
+int fwi_apply_random_boundary(fwi_ctx *c, const fwi_rbc *rbc, uint64_t seed)
+{
+    if (!c || !rbc) return FWI_ERR_ARG;
+    return guarded(c, [&] {
+        if (!c->have_vp) fail(FWI_ERR_STATE, "no velocity model set");
+        if (rbc->kind != 0 && rbc->kind != 1) fail(FWI_ERR_ARG, "unknown random boundary kind %d", rbc->kind);
+        const double cap = (rbc->cfl_cap > 0 ? rbc->cfl_cap : 0.98) * stability_velocity(c->g.dh, c->p.dt);
+        float vlo, vhi;
+        if (rbc->kind == 0) {
+            vlo = c->vmin - rbc->varVp;
+            vhi = (float)std::min<double>(c->vmax + rbc->varVp, cap);
+            vlo = std::max(vlo, 0.05f * c->vmin);
+        } else {
+            vlo = 0.05f * c->vmin;
+            vhi = (float)cap;
+        }
+        // always start from the clean padded model (no drift between shots)
+        CK(cudaMemcpyAsync(c->vp.p, c->vp_clean.p, c->vol * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
+        rbc_background_kernel<<<grid_blocks(c->vol), 256, 0, c->stream>>>(
+            c->vp.p, c->nzz, c->nxx, c->nyy, c->ldz, c->g.nb, rbc->kind, rbc->ratio, rbc->varVp, vlo, vhi, seed);
+        CK(cudaGetLastError());
+        c->launches += 1;
+        if (rbc->kind == 0 && rbc->ratio > 0 && rbc->varVp > 0) {
+            const float dh = c->g.dh;
+            const float xm = (c->nxx - 1) * dh, ym = (c->nyy - 1) * dh, zm = (c->nzz - 1) * dh;
+            std::mt19937_64 rng(splitmix64(seed ^ 0x5EEDB10Bull));
+            std::vector<float> pts = poisson_points(xm, ym, zm, rbc->ratio, rng);
+            const float fnb = c->g.nb * dh;
+            std::vector<Blob> blobs;
+            std::uniform_real_distribution<float> U(0.0f, 1.0f);
+            for (size_t q = 0; q < pts.size() / 3; ++q) {
+                const float x = pts[3 * q], y = pts[3 * q + 1], z = pts[3 * q + 2];
+                if (x > 0.5f * fnb && x < xm - 0.5f * fnb && y > 0.5f * fnb && y < ym - 0.5f * fnb &&
+                    z > 0.5f * fnb && z < zm - 0.5f * fnb)
+                    continue;
+                Blob b;
+                b.x = x;
+                b.y = y;
+                b.z = z;
+                b.r = rbc->ratio * (0.2f + 0.8f * U(rng));
+                const float A = rbc->varVp * (0.5f + 0.5f * U(rng));
+                b.amp = ((rng() % 3) == 0 ? -1.0f : 1.0f) * A;
+                blobs.push_back(b);
+            }
+            if (!blobs.empty()) {
+                const float bin = 5.0f * rbc->ratio;
+                const int nbz = (int)(zm / bin) + 1, nbx = (int)(xm / bin) + 1, nby = (int)(ym / bin) + 1;
+                std::vector<std::vector<int>> bins((size_t)nbz * nbx * nby);
+                for (size_t q = 0; q < blobs.size(); ++q) {
+                    const Blob &b = blobs[q];
+                    const float e = 5.0f * b.r;
+                    auto lo = [&](float v, int nbn) { return std::max(0, std::min(nbn - 1, (int)std::floor((v - e) / bin))); };
+                    auto hi = [&](float v, int nbn) { return std::max(0, std::min(nbn - 1, (int)std::floor((v + e) / bin))); };
+                    for (int by = lo(b.y, nby); by <= hi(b.y, nby); ++by)
+                        for (int bx = lo(b.x, nbx); bx <= hi(b.x, nbx); ++bx)
+                            for (int bz = lo(b.z, nbz); bz <= hi(b.z, nbz); ++bz)
+                                bins[bz + (size_t)nbz * (bx + (size_t)nbx * by)].push_back((int)q);
+                }
+                std::vector<int> first(1, 0), list;
+                for (auto &v : bins) {
+                    list.insert(list.end(), v.begin(), v.end());
+                    first.push_back((int)list.size());
+                }
+                DevBuf<Blob> db;
+                DevBuf<int> dfirst, dlist;
+                db.ensure(blobs.size());
+                dfirst.ensure(first.size());
+                dlist.ensure(std::max<size_t>(list.size(), 1));
+                cudaError_t e = cudaMemcpyAsync(db.p, blobs.data(), blobs.size() * sizeof(Blob), cudaMemcpyHostToDevice, c->stream);
+                if (e == cudaSuccess) e = cudaMemcpyAsync(dfirst.p, first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream);
+                if (e == cudaSuccess && !list.empty()) e = cudaMemcpyAsync(dlist.p, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream);
+                if (e == cudaSuccess) {
+                    rbc_blobs_kernel<<<grid_blocks(c->vol), 256, 0, c->stream>>>(
+                        c->vp.p, c->nzz, c->nxx, c->nyy, c->ldz, c->g.nb, dh, db.p, dfirst.p, dlist.p, nbz, nbx, nby,
+                        bin, vlo, vhi);
+                    e = cudaGetLastError();
+                }
+                if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+                db.release();
+                dfirst.release();
+                dlist.release();
+                CK(e);
+                c->launches += 1;
+            }
+        }
+        check_cfl(c);
+    });
+}
+
+int fwi_set_geometry(fwi_ctx *c, int nsrc, const float *sx, const float *sy, const float *sz, int nrec,
+                     const float *rx, const float *ry, const float *rz, const int *rec_first, const int *rec_count)
+{
+    if (!c || nsrc < 0 || nrec < 0 || (nsrc && (!sx || !sy || !sz)) || (nrec && (!rx || !ry || !rz)))
+        return FWI_ERR_ARG;
+    return guarded(c, [&] {
+        const float dh = c->g.dh;
+        const int nb = c->g.nb;
+        auto inside = [&](int i, int j, int k) {
+            return i >= 4 && i < c->nzz - 4 && j >= 4 && j < c->nxx - 4 && k >= 4 && k < c->nyy - 4;
+        };
+        std::vector<int> s(3 * nsrc), r(3 * nrec), f(nsrc), n(nsrc);
+        for (int q = 0; q < nsrc; ++q) {
+            s[3 * q] = grid_index(sz[q], dh, nb);
+            s[3 * q + 1] = grid_index(sx[q], dh, nb);
+            s[3 * q + 2] = grid_index(sy[q], dh, nb);
+            if (!inside(s[3 * q], s[3 * q + 1], s[3 * q + 2]))
+                fail(FWI_ERR_ARG, "source %d at (%g,%g,%g) m falls outside the updated grid", q, sx[q], sy[q], sz[q]);
+        }
+        for (int q = 0; q < nrec; ++q) {
+            r[3 * q] = grid_index(rz[q], dh, nb);
+            r[3 * q + 1] = grid_index(rx[q], dh, nb);
+            r[3 * q + 2] = grid_index(ry[q], dh, nb);
+            if (!inside(r[3 * q], r[3 * q + 1], r[3 * q + 2]))
+                fail(FWI_ERR_ARG, "receiver %d at (%g,%g,%g) m falls outside the updated grid", q, rx[q], ry[q], rz[q]);
+        }
+        for (int q = 0; q < nsrc; ++q) {
+            f[q] = rec_first ? rec_first[q] : 0;
+            n[q] = rec_count ? rec_count[q] : nrec;
+            if (f[q] < 0 || n[q] < 0 || f[q] + n[q] > nrec) fail(FWI_ERR_ARG, "shot %d receiver range out of bounds", q);
+        }
+        c->sijk = std::move(s);
+        c->rijk = std::move(r);
+        c->rfirst = std::move(f);
+        c->rcount = std::move(n);
+        c->nsrc = nsrc;
+        c->nrec = nrec;
+        c->have_geom = true;
+    });
+}
+
+int fwi_shot_nrec(fwi_ctx *c, int shot, int *nrec)
+{
+    if (!c || !nrec || shot < 0 || shot >= c->nsrc) return FWI_ERR_ARG;
+    *nrec = c->rcount[shot];
+    return FWI_OK;
+}
+
+int fwi_model_shots(fwi_ctx *c, const int *shots, int n, float *seis)
+{
+    if (!c || !shots || n < 0 || (n && !seis)) return FWI_ERR_ARG;
+    return guarded(c, [&] { model_impl(c, shots, n, seis, false); });
+}
+
+int fwi_model_shots_dev(fwi_ctx *c, const int *shots, int n, float *d_seis)
+{
+    if (!c || !shots || n < 0 || (n && !d_seis)) return FWI_ERR_ARG;
+    return guarded(c, [&] { model_impl(c, shots, n, d_seis, true); });
+}
+
+int fwi_rtm_shots(fwi_ctx *c, const int *shots, int n, const float *data)
+{
+    if (!c || !shots || n < 0 || (n && !data)) return FWI_ERR_ARG;
+    return guarded(c, [&] { migrate_impl(c, shots, n, data, false, false); });
+}
+
+int fwi_rtm_shots_dev(fwi_ctx *c, const int *shots, int n, const float *d_data)
+{
+    if (!c || !shots || n < 0 || (n && !d_data)) return FWI_ERR_ARG;
+    return guarded(c, [&] { migrate_impl(c, shots, n, d_data, true, false); });
+}
+
+int fwi_gradient_shots(fwi_ctx *c, const int *shots, int n, const float *res)
+{
+    if (!c || !shots || n < 0 || (n && !res)) return FWI_ERR_ARG;
+    return guarded(c, [&] { migrate_impl(c, shots, n, res, false, true); });
+}
+
+int fwi_gradient_shots_dev(fwi_ctx *c, const int *shots, int n, const float *d_res)
+{
+    if (!c || !shots || n < 0 || (n && !d_res)) return FWI_ERR_ARG;
+    return guarded(c, [&] { migrate_impl(c, shots, n, d_res, true, true); });
+}
+
+int fwi_reset_accumulators(fwi_ctx *c)
+{
+    if (!c) return FWI_ERR_ARG;
+    return guarded(c, [&] {
+        ensure_fields(c, true);
+        const size_t bytes = (size_t)c->B * c->vol * sizeof(float);
+        CK(cudaMemsetAsync(c->acc_img.p, 0, bytes, c->stream));
+        CK(cudaMemsetAsync(c->acc_ill.p, 0, bytes, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        c->acc_dirty = false;
+    });
+}
+
+int fwi_get_accumulators(fwi_ctx *c, float *img, float *ill)
+{
+    if (!c) return FWI_ERR_ARG;
+    return guarded(c, [&] {
+        fold_accumulators(c);
+        const size_t n = (size_t)c->nzz * c->nxx * c->nyy;
+        c->post.ensure(n);
+        float *outs[2] = {img, ill};
+        const float *srcs[2] = {c->acc_img.p, c->acc_ill.p};
+        for (int q = 0; q < 2; ++q) {
+            if (!outs[q]) continue;
+            pitched_to_dense_kernel<<<grid_blocks(n), 256, 0, c->stream>>>(srcs[q], c->nzz, c->nxx, c->nyy, c->ldz,
+                                                                           c->post.p);
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(outs[q], c->post.p, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+            c->launches += 1;
+        }
+    });
+}
+
+int fwi_get_accumulators_dev(fwi_ctx *c, float *d_img, float *d_ill)
+{
+    if (!c) return FWI_ERR_ARG;
+    return guarded(c, [&] {
+        fold_accumulators(c);
+        const size_t n = (size_t)c->nzz * c->nxx * c->nyy;
+        float *outs[2] = {d_img, d_ill};
+        const float *srcs[2] = {c->acc_img.p, c->acc_ill.p};
+        for (int q = 0; q < 2; ++q) {
+            if (!outs[q]) continue;
+            pitched_to_dense_kernel<<<grid_blocks(n), 256, 0, c->stream>>>(srcs[q], c->nzz, c->nxx, c->nyy, c->ldz,
+                                                                           outs[q]);
+            CK(cudaGetLastError());
+            c->launches += 1;
+        }
+        CK(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int fwi_set_accumulators_dev(fwi_ctx *c, const float *d_img, const float *d_ill)
+{
+    if (!c) return FWI_ERR_ARG;
+    return guarded(c, [&] {
+        ensure_fields(c, true);
+        fold_accumulators(c);
+        const float *ins[2] = {d_img, d_ill};
+        float *dsts[2] = {c->acc_img.p, c->acc_ill.p};
+        for (int q = 0; q < 2; ++q) {
+            if (!ins[q]) continue;
+            dense_to_pitched_kernel<<<grid_blocks(c->vol), 256, 0, c->stream>>>(ins[q], c->nzz, c->nxx, c->nyy,
+                                                                                c->ldz, dsts[q]);
+            CK(cudaGetLastError());
+            c->launches += 1;
+        }
+        CK(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int fwi_rtm_image(fwi_ctx *c, float *image)
+{
+    if (!c || !image) return FWI_ERR_ARG;
+    return guarded(c, [&] {
+        fold_accumulators(c);
+        const long long n = (long long)c->g.nz * c->g.nx * c->g.ny;
+        c->post.ensure(std::max<size_t>(n, (size_t)c->nzz * c->nxx * c->nyy));
+        rtm_image_kernel<<<grid_blocks(n), 256, 0, c->stream>>>(c->acc_img.p, c->acc_ill.p, c->g.nz, c->g.nx, c->g.ny,
+                                                                c->g.nb, c->nxx, c->ldz, c->idh2, c->post.p);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(image, c->post.p, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        c->launches += 1;
+    });
+}
+
+int fwi_gradient_post(fwi_ctx *c, float zmask, float *grad, float *gmax)
+{
+    if (!c || !grad) return FWI_ERR_ARG;
+    return guarded(c, [&] {
+        fold_accumulators(c);
+        const long long n = (long long)c->g.nz * c->g.nx * c->g.ny;
+        c->post.ensure(std::max<size_t>(n, (size_t)c->nzz * c->nxx * c->nyy));
+        c->ubits.ensure(1);
+        CK(cudaMemsetAsync(c->ubits.p, 0, sizeof(unsigned), c->stream));
+        const int imask = (int)(zmask / c->g.dh);
+        grad_post_kernel<<<grid_blocks(n), 256, 0, c->stream>>>(c->acc_img.p, c->acc_ill.p, c->g.nz, c->g.nx, c->g.ny,
+                                                                c->g.nb, c->nxx, c->ldz, c->idh2, imask, c->post.p,
+                                                                c->ubits.p);
+        scale_by_inverse_kernel<<<grid_blocks(n), 256, 0, c->stream>>>(c->post.p, n, c->ubits.p);
+        CK(cudaGetLastError());
+        c->launches += 2;
+        unsigned bits = 0;
+        CK(cudaMemcpyAsync(&bits, c->ubits.p, sizeof bits, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(grad, c->post.p, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (gmax) memcpy(gmax, &bits, sizeof(float));
+    });
+}
+
+int fwi_residual(fwi_ctx *c, const float *obs, const float *cal, int64_t n, float *res, double *sum_sq)
+{
+    if (!c || !obs || !cal || n < 0 || !sum_sq) return FWI_ERR_ARG;
+    return guarded(c, [&] {
+        DevBuf<float> d;
+        d.ensure(3 * (size_t)std::max<int64_t>(n, 1));
+        cudaError_t e = cudaMemcpyAsync(d.p, obs, n * sizeof(float), cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d.p + n, cal, n * sizeof(float), cudaMemcpyHostToDevice, c->stream);
+        if (e != cudaSuccess) {
+            d.release();
+            CK(e);
+        }
+        try {
+            *sum_sq = residual_impl(c, d.p, d.p + n, n, res ? d.p + 2 * n : nullptr);
+            if (res) CK(cudaMemcpy(res, d.p + 2 * n, n * sizeof(float), cudaMemcpyDeviceToHost));
+        } catch (...) {
+            d.release();
+            throw;
+        }
+        d.release();
+    });
+}
+
+int fwi_residual_dev(fwi_ctx *c, const float *d_obs, const float *d_cal, int64_t n, float *d_res, double *sum_sq)
+{
+    if (!c || !d_obs || !d_cal || n < 0 || !sum_sq) return FWI_ERR_ARG;
+    return guarded(c, [&] { *sum_sq = residual_impl(c, d_obs, d_cal, n, d_res); });
+}
+
+int fwi_dot_dev(fwi_ctx *c, const float *a, const float *b, int64_t n, double *out)
+{
+    if (!c || !a || !b || n < 0 || !out) return FWI_ERR_ARG;
+    return guarded(c, [&] {
+        c->partial.ensure(kRedBlocks);
+        c->dsum.ensure(1);
+        dot_partial_kernel<kRedThreads><<<kRedBlocks, kRedThreads, 0, c->stream>>>(a, b, n, c->partial.p);
+        finish_sum_kernel<kRedThreads><<<1, kRedThreads, 0, c->stream>>>(c->partial.p, kRedBlocks, c->dsum.p);
+        CK(cudaGetLastError());
+        c->launches += 2;
+        CK(cudaMemcpyAsync(out, c->dsum.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int fwi_last_timing(fwi_ctx *c, float *fwd_ms, float *bwd_ms)
+{
+    if (!c) return FWI_ERR_ARG;
+    if (fwd_ms) *fwd_ms = c->fwd_ms;
+    if (bwd_ms) *bwd_ms = c->bwd_ms;
+    return FWI_OK;
+}
+
+int fwi_launch_count(fwi_ctx *c, int64_t *count)
+{
+    if (!c || !count) return FWI_ERR_ARG;
+    *count = c->launches;
+    return FWI_OK;
+}
+
+int fwi_get_tiles(fwi_ctx *c, int *f, int *b)
+{
+    if (!c) return FWI_ERR_ARG;
+    if (f) *f = c->tile_fwd;
+    if (b) *b = c->tile_bwd;
+    return FWI_OK;
+}
+
+int fwi_set_tiles(fwi_ctx *c, int f, int b)
+{
+    if (!c || f < -1 || f >= kNumTiles || b < -1 || b >= kNumTiles) return FWI_ERR_ARG;
+    c->tile_fwd = f;
+    c->tile_bwd = b;
+    return FWI_OK;
+}
+
+// Time every compiled tile (and two y-chunk counts) on a few steps of the
+// context's own fields and keep the fastest for each kernel.
+int fwi_autotune(fwi_ctx *c)
+{
+    if (!c) return FWI_ERR_ARG;
+    return guarded(c, [&] {
+        require_ready(c);
+        const bool adj = c->p.boundary == FWI_BOUNDARY_RBC;
+        ensure_fields(c, adj);
+        std::vector<int> one(1, 0);
+        BatchTables t = build_batch(c, one.data(), 1);
+        t.info.nshot = c->B;  // every slot busy, like a full batch
+        for (int s = 1; s < c->B; ++s)
+            for (int a = 0; a < 3; ++a) t.info.src[s][a] = t.info.src[0][a];
+        t.info.R = 0;
+        t.info.ncell = 0;
+        upload_batch(c, t);
+        const int steps = 6;
+        cudaEvent_t e0, e1;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        float best = 1e30f;
+        int best_tile = 0, best_chunk = 1;
+        for (int tile = 0; tile < kNumTiles; ++tile) {
+            KInfo k = fwd_kernel(tile, !adj);
+            const int base = default_chunks(c, k, c->B);
+            for (int nchunk : {base, std::max(1, base / 2), base * 2}) {
+                FwdLaunch L = make_fwd(c, c->B, tile, nchunk, false);
+                launch_fwd(c, L, 0, 0);
+                CK(cudaEventRecord(e0, c->stream));
+                for (int s = 0; s < steps; ++s) launch_fwd(c, L, 1, s & 1);
+                CK(cudaEventRecord(e1, c->stream));
+                CK(cudaEventSynchronize(e1));
+                float ms = 0;
+                CK(cudaEventElapsedTime(&ms, e0, e1));
+                c->launches += steps + 1;
+                if (ms < best) {
+                    best = ms;
+                    best_tile = tile;
+                    best_chunk = nchunk;
+                }
+            }
+        }
+        c->tile_fwd = best_tile;
+        c->chunk_fwd = best_chunk;
+        if (adj) {
+            best = 1e30f;
+            best_tile = 0;
+            best_chunk = 1;
+            for (int tile = 0; tile < kNumTiles; ++tile) {
+                KInfo k = bwd_kernel(tile, false, false);
+                const int base = default_chunks(c, k, c->B);
+                for (int nchunk : {base, std::max(1, base / 2), base * 2}) {
+                    BwdLaunch L = make_bwd(c, c->B, tile, nchunk, false);
+                    launch_bwd(c, L, 0, 0, 0);
+                    CK(cudaEventRecord(e0, c->stream));
+                    for (int s = 0; s < steps; ++s) launch_bwd(c, L, 1, s & 1, s & 1);
+                    CK(cudaEventRecord(e1, c->stream));
+                    CK(cudaEventSynchronize(e1));
+                    float ms = 0;
+                    CK(cudaEventElapsedTime(&ms, e0, e1));
+                    c->launches += steps + 1;
+                    if (ms < best) {
+                        best = ms;
+                        best_tile = tile;
+                        best_chunk = nchunk;
+                    }
+                }
+            }
+            c->tile_bwd = best_tile;
+            c->chunk_bwd = best_chunk;
+            // tuning ran the imaging condition on scratch data
+            const size_t bytes = (size_t)c->B * c->vol * sizeof(float);
+            CK(cudaMemsetAsync(c->acc_img.p, 0, bytes, c->stream));
+            CK(cudaMemsetAsync(c->acc_ill.p, 0, bytes, c->stream));
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        check_status(c);
+    });
+}
+
+}  // extern "C"

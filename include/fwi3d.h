@@ -1,0 +1,192 @@
+/*
+ * fwi3d.h -- C ABI of the B200 wave-propagation library (libfwi3d.so).
+ *
+ * The library replaces the device side of FWI3D's three workflows:
+ *   src/modeling  (class Modeling:  forward_solver / get_seismogram)
+ *   src/migration (class Migration: forward_propagation / backward_propagation /
+ *                  export_seismic)
+ *   src/inversion (class Inversion: compute_gradient / optimization /
+ *                  update_model)
+ * All paths in citations are inside phbastosa/FWI3D.
+ *
+ * Conventions
+ *   - Volumes are float32, z fastest, then x, then y (Fortran [nz, nx, ny]),
+ *     as read by src/modeling/modeling.cu:160-162 and written by
+ *     src/migration/migration.cu:162-163.
+ *   - Seismograms are float32 Fortran [nt, nrec] (sample t of receiver r at
+ *     t + r*nt), as written by src/modeling/modeling.cu:302-307.
+ *   - Host buffers are owned by the caller; device buffers by the library.
+ *     Entry points ending in _dev take device pointers instead.
+ *   - Every call returns an int status (FWI_OK = 0).  No C++ exception crosses
+ *     the ABI.  fwi_last_error() returns the message of the last failure.
+ *   - One context per host thread; calls on one context are not re-entrant.
+ *     Each context owns one CUDA stream (or uses the one set with
+ *     fwi_set_stream) and its captured time-loop graphs.
+ */
+#ifndef FWI3D_H
+#define FWI3D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define FWI_OK 0
+#define FWI_ERR_ARG 1       /* bad argument or size */
+#define FWI_ERR_CUDA 2      /* CUDA runtime / driver error */
+#define FWI_ERR_ALLOC 3     /* device allocation failed */
+#define FWI_ERR_TIMEOUT 4   /* a bounded device wait gave up */
+#define FWI_ERR_STATE 5     /* call out of order (e.g. no velocity yet) */
+#define FWI_ERR_IO 6        /* file could not be opened (host helpers) */
+#define FWI_ERR_NUMERIC 7   /* CFL violated or non-finite result */
+#define FWI_ERR_NODEV 8     /* no CUDA device */
+
+/* boundary treatment of the padded grid */
+#define FWI_BOUNDARY_ABC 0  /* Cerjan sponge, src/modeling/modeling.cu:83-140, 395-520 */
+#define FWI_BOUNDARY_RBC 1  /* random velocity pad, no damping, modeling.cu:558-673 */
+
+/* behaviour flags (fwi_params.flags) */
+#define FWI_FLAG_GRAD_DY 0x1        /* include d2/dy2 in the gradient (reference omits it,
+                                       src/inversion/inversion.cu:557) */
+#define FWI_FLAG_SUBTRACT_SOURCE 0x2 /* remove the source while rebuilding the forward field
+                                       backwards (reference does not, migration.cu:242) */
+
+typedef struct fwi_ctx fwi_ctx;
+
+/* Grid: the unpadded model plus the pad width.
+ * Replaces Modeling::set_main_parameters / set_properties
+ * (src/modeling/modeling.cu:17-34, 142-179) and Migration/Inversion's
+ * nb = int(length/dh)+1 (src/migration/migration.cu:60, inversion.cu:148,175). */
+typedef struct {
+    int nz, nx, ny;   /* z_samples, x_samples, y_samples */
+    int nb;           /* pad cells on every side */
+    float dh;         /* model_spacing [m] */
+} fwi_grid;
+
+/* Time axis and boundary. fmax is max_frequency: the Ricker peak is fmax/3
+ * (src/modeling/modeling.cu:36-59). */
+typedef struct {
+    int nt;            /* time_samples */
+    float dt;          /* time_spacing [s] */
+    float fmax;        /* max_frequency [Hz] */
+    int boundary;      /* FWI_BOUNDARY_ABC or FWI_BOUNDARY_RBC */
+    float abc_factor;  /* abc_factor (used with FWI_BOUNDARY_ABC) */
+    int max_batch;     /* shots propagated together in one launch (>= 1) */
+    int flags;         /* FWI_FLAG_* */
+} fwi_params;
+
+/* Random-boundary recipe. kind 0 follows the reference
+ * (src/modeling/modeling.cu:558-673: ramped Gaussian noise per pad axis plus
+ * Gaussian blobs on Poisson-disk points, clamped to [vmin-varVp, vmax+varVp]);
+ * kind 1 is a ramped uniform relative perturbation (|dv/v| <= ratio at the
+ * outer face).  Both are deterministic functions of the seed and both cap the
+ * pad at cfl_cap * the leapfrog stability velocity. */
+typedef struct {
+    int kind;          /* 0 = reference recipe, 1 = uniform relative */
+    float ratio;       /* kind 0: blob radius scale [m] (rbc_ratio); kind 1: max |dv/v| */
+    float varVp;       /* kind 0: velocity spread [m/s] (rbc_varVp) */
+    float cfl_cap;     /* fraction of the stability limit (<= 0: 0.98) */
+} fwi_rbc;
+
+/* ---- lifetime ---------------------------------------------------------- */
+int fwi_create(const fwi_grid *grid, const fwi_params *params, fwi_ctx **out);
+int fwi_destroy(fwi_ctx *ctx);
+const char *fwi_status_string(int status);
+int fwi_last_error(fwi_ctx *ctx, char *buf, int buflen);
+/* Run the context's work on a caller stream (cudaStream_t as void*). */
+int fwi_set_stream(fwi_ctx *ctx, void *stream);
+/* Padded dims, device pitch and time lag the context uses. */
+int fwi_get_dims(fwi_ctx *ctx, int *nzz, int *nxx, int *nyy, int *ldz, int *tlag);
+
+/* ---- model ------------------------------------------------------------- */
+/* Unpadded model [nz,nx,ny]; padded on the GPU by edge replication
+ * (replaces expand_boundary, src/modeling/modeling.cu:181-228). */
+int fwi_set_velocity(fwi_ctx *ctx, const float *vp);
+/* Padded model [nzz,nxx,nyy] as is (parity harnesses inject identical pads). */
+int fwi_set_padded_velocity(fwi_ctx *ctx, const float *vp_padded);
+int fwi_get_padded_velocity(fwi_ctx *ctx, float *vp_padded);
+/* Overwrite the pad with a random boundary (replaces set_random_boundary,
+ * src/modeling/modeling.cu:558-592).  Deterministic in (seed). */
+int fwi_apply_random_boundary(fwi_ctx *ctx, const fwi_rbc *rbc, uint64_t seed);
+
+/* ---- geometry ---------------------------------------------------------- */
+/* Source and receiver coordinates in metres (SPS/RPS, src/geometry/
+ * geometry.cpp:3-47); grid index = int((c + dh/2)/dh) + nb
+ * (src/modeling/modeling.cu:264-300).  rec_first/rec_count give each shot
+ * its receiver range inside rx/ry/rz; NULL means every shot uses all nrec. */
+int fwi_set_geometry(fwi_ctx *ctx, int nsrc, const float *sx, const float *sy, const float *sz,
+                     int nrec, const float *rx, const float *ry, const float *rz,
+                     const int *rec_first, const int *rec_count);
+int fwi_shot_nrec(fwi_ctx *ctx, int shot, int *nrec);
+
+/* ---- modeling ---------------------------------------------------------- */
+/* Forward-model shots; seismograms are written one after another, shot s as
+ * Fortran [nt, nrec_s].  Replaces Modeling::forward_solver + get_seismogram
+ * (src/modeling/modeling.cu:302-322, 324-393). */
+int fwi_model_shots(fwi_ctx *ctx, const int *shots, int nshots, float *seis);
+int fwi_model_shots_dev(fwi_ctx *ctx, const int *shots, int nshots, float *d_seis);
+
+/* ---- migration --------------------------------------------------------- */
+/* Forward through the current (random-boundary) model, then the fused pass:
+ * rebuild the source field backwards, propagate the time-reversed data and
+ * accumulate image += Ps*Pr, illum += Ps^2.  data holds each shot's
+ * [nt, nrec_s] seismogram one after another.  Replaces
+ * Migration::forward_propagation + backward_propagation
+ * (src/migration/migration.cu:96-128, 166-248). */
+int fwi_rtm_shots(fwi_ctx *ctx, const int *shots, int nshots, const float *data);
+int fwi_rtm_shots_dev(fwi_ctx *ctx, const int *shots, int nshots, const float *d_data);
+/* Zero the padded image / gradient and illumination accumulators. */
+int fwi_reset_accumulators(fwi_ctx *ctx);
+/* Raw padded accumulators [nzz,nxx,nyy] (either pointer may be NULL). */
+int fwi_get_accumulators(fwi_ctx *ctx, float *image_padded, float *illum_padded);
+/* Same, into caller device buffers [nzz,nxx,nyy] (for a cross-GPU sum of
+ * shot-sharded images before the post-processing). */
+int fwi_get_accumulators_dev(fwi_ctx *ctx, float *d_image_padded, float *d_illum_padded);
+/* Replace the accumulators by caller device buffers [nzz,nxx,nyy] (after
+ * such a sum, or to resume from a saved image). */
+int fwi_set_accumulators_dev(fwi_ctx *ctx, const float *d_image_padded, const float *d_illum_padded);
+/* Final image [nz,nx,ny]: crop, divide by illumination, -d2/dz2
+ * (replaces Migration::export_seismic, src/migration/migration.cu:137-164). */
+int fwi_rtm_image(fwi_ctx *ctx, float *image);
+
+/* ---- inversion --------------------------------------------------------- */
+/* Same fused pass with the gradient imaging condition
+ * grad += dt*Pr*(d2x+d2z[+d2y])Ps*v^2 (src/inversion/inversion.cu:491-558);
+ * residual holds each shot's [nt, nrec_s] obs-cal one after another. */
+int fwi_gradient_shots(fwi_ctx *ctx, const int *shots, int nshots, const float *residual);
+int fwi_gradient_shots_dev(fwi_ctx *ctx, const int *shots, int nshots, const float *d_residual);
+/* Gradient post-processing [nz,nx,ny]: crop, divide by illumination, -d2/dz2
+ * below int(zmask/dh), divide by max|g| (src/inversion/inversion.cu:233-260).
+ * gmax receives max|g| before normalisation (may be NULL). */
+int fwi_gradient_post(fwi_ctx *ctx, float zmask, float *grad, float *gmax);
+/* Residual obs - cal and its sum of squares, accumulated in FP64 on the GPU
+ * (replaces the FP32 host loop of src/inversion/inversion.cu:281-292).
+ * res may be NULL. */
+int fwi_residual(fwi_ctx *ctx, const float *obs, const float *cal, int64_t n, float *res,
+                 double *sum_sq);
+int fwi_residual_dev(fwi_ctx *ctx, const float *d_obs, const float *d_cal, int64_t n,
+                     float *d_res, double *sum_sq);
+/* FP64 dot product of two device vectors (gradient dot products). */
+int fwi_dot_dev(fwi_ctx *ctx, const float *d_a, const float *d_b, int64_t n, double *out);
+
+/* ---- diagnostics ------------------------------------------------------- */
+/* Device time [ms] of the last call's forward and backward time loops. */
+int fwi_last_timing(fwi_ctx *ctx, float *fwd_ms, float *bwd_ms);
+/* Kernel launches issued by the library since creation (graph nodes count
+ * once per replay). */
+int fwi_launch_count(fwi_ctx *ctx, int64_t *count);
+/* Stencil tile chosen by the autotuner for the forward and backward kernels
+ * (index into the compiled tile table; -1 = not tuned yet). */
+int fwi_get_tiles(fwi_ctx *ctx, int *fwd_tile, int *bwd_tile);
+int fwi_set_tiles(fwi_ctx *ctx, int fwd_tile, int bwd_tile);
+int fwi_autotune(fwi_ctx *ctx);
+int fwi_num_tiles(int *n);
+int fwi_tile_shape(int tile, int *tz, int *tx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FWI3D_H */
