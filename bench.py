@@ -179,7 +179,11 @@ def run_ours(args, ws, rank, local):
     ctx.set_stream(stream.cuda_stream)
     ctx.set_geometry(w.src, w.rec, w.rec_first, w.rec_count)
     ctx.set_velocity(w.start if w.start is not None else w.vp)
-    ctx.autotune()
+    if args.tiles:
+        f, b = (int(x) for x in args.tiles.split(","))
+        ctx.set_tiles(f, b)
+    else:
+        ctx.autotune()
     nsrc = len(w.src)
     N = ctx.tlag + w.nt
     cells = ctx.nzz * ctx.nxx * ctx.nyy
@@ -196,6 +200,7 @@ def run_ours(args, ws, rank, local):
     if not rtm:
         seis_dev = torch.empty(max(ctx.shot_nrec(s) for s in range(nsrc)) * w.nt, device="cuda")
     rbc = dict(w.rbc)
+    torch.cuda.synchronize()  # data come from the default stream; the library runs on `stream`
 
     def step(s, timing):
         ctx.apply_random_boundary(seed=1000 + s, **rbc)
@@ -269,7 +274,7 @@ def run_ours(args, ws, rank, local):
 
     # end to end through the public API with host buffers
     e2e = None
-    if rank == 0 or ws > 1:
+    if not args.no_e2e:
         host = {}
         for s in set(shots[args.warmup:]):
             n = (ctx.shot_nrec(s) * w.nt)
@@ -395,6 +400,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["rtm", "modeling"], default="rtm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
+    ap.add_argument("--tiles", default="", help="fixed forward,backward tile indices instead of autotuning")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     if args.impl == "reference":
