@@ -57,7 +57,7 @@ def build_library(force: bool = False, verbose: bool = False, ptxas_info: bool =
     LIB_DIR.mkdir(exist_ok=True)
     srcs = sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "fwi3d.h"]
     if force or ptxas_info or _stale(LIB, srcs):
-        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-shared", "-o", str(LIB), str(CSRC / "fwi3d.cu")]
+        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-shared", "-o", str(LIB), *map(str, sorted(CSRC.glob("*.cu")))]
         if ptxas_info:
             cmd.insert(1, "-Xptxas=-v")
         _run(cmd, verbose)

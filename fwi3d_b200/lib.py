@@ -65,6 +65,7 @@ SIGNATURES = {
     "fwi_gradient_post": (_i, [_p, _f, _fp, _fp]),
     "fwi_residual": (_i, [_p, _fp, _fp, _i64, _fp, _dp]),
     "fwi_residual_dev": (_i, [_p, _p, _p, _i64, _p, _dp]),
+    "fwi_residual_noalloc": (_i, [_p, _p, _i64, _p, _p, _p]),
     "fwi_dot_dev": (_i, [_p, _p, _p, _i64, _dp]),
     "fwi_last_timing": (_i, [_p, _fp, _fp]),
     "fwi_launch_count": (_i, [_p, C.POINTER(C.c_int64)]),
@@ -346,6 +347,18 @@ class Context:
 
     def set_tiles(self, fwd: int, bwd: int):
         self._check(self.lib.fwi_set_tiles(self.h, fwd, bwd))
+
+
+NOALLOC_MAX_N = 268435456
+
+
+def residual_noalloc(d_obs: int, d_cal: int, n: int, d_res: int, d_sum_sq: int, stream: int = 0) -> None:
+    """fwi_residual_noalloc on caller device buffers (no context, no device
+    allocation); the FP64 sum lands in the double at d_sum_sq."""
+    st = load().fwi_residual_noalloc(C.c_void_p(d_obs), C.c_void_p(d_cal), n, C.c_void_p(d_res or None),
+                                     C.c_void_p(d_sum_sq), C.c_void_p(stream or None))
+    if st != FWI_OK:
+        raise FwiError(st, "fwi_residual_noalloc failed (n above NOALLOC_MAX_N or a CUDA error)")
 
 
 def tile_table() -> list[tuple[int, int]]:

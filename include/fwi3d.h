@@ -169,6 +169,19 @@ int fwi_residual(fwi_ctx *ctx, const float *obs, const float *cal, int64_t n, fl
                  double *sum_sq);
 int fwi_residual_dev(fwi_ctx *ctx, const float *d_obs, const float *d_cal, int64_t n,
                      float *d_res, double *sum_sq);
+/* No counterpart in the reference.  The residual and FP64 sum of squares of
+ * fwi_residual_dev for callers that cannot let a library allocate device
+ * memory (a latency-critical loop that cannot absorb cudaMalloc's implicit
+ * device synchronisation, or an application whose own pool owns all device
+ * memory).  Needs no context: d_obs, d_cal, d_res (may be NULL) and d_sum_sq
+ * (one double) are caller device buffers; stream may be NULL.  The scratch is
+ * a fixed 32 KiB device array inside the library, so n <= FWI_NOALLOC_MAX_N
+ * (larger n returns FWI_ERR_ARG); every call on a device shares it, so calls
+ * that overlap on the GPU race.  The first call on a device looks the array up
+ * and should come before any stream capture. */
+#define FWI_NOALLOC_MAX_N 268435456LL
+int fwi_residual_noalloc(const float *d_obs, const float *d_cal, int64_t n, float *d_res,
+                         double *d_sum_sq, void *stream);
 /* FP64 dot product of two device vectors (gradient dot products). */
 int fwi_dot_dev(fwi_ctx *ctx, const float *d_a, const float *d_b, int64_t n, double *out);
 
