@@ -189,8 +189,10 @@ def run_ours(args, ws, rank, local):
     cells = ctx.nzz * ctx.nxx * ctx.nyy
     updates_per_step = cells * N * (3 if rtm else 1)
 
+    from fwi3d_b200 import shots as shotlib
     total = args.warmup + args.steps
-    shots = [(rank + ws * k) % nsrc for k in range(total)]
+    mine = shotlib.partition(nsrc, ws, rank)
+    shots = [mine[k % len(mine)] for k in range(total)]
     g = torch.Generator(device="cuda").manual_seed(1234 + rank)
     data = {}
     if rtm:
@@ -231,11 +233,7 @@ def run_ours(args, ws, rank, local):
             for k in range(args.warmup, total):
                 step(shots[k], timing)
             if img_all is not None:
-                import torch.distributed as dist
-                ctx.get_accumulators_dev(img_all.data_ptr(), ill_all.data_ptr())
-                dist.all_reduce(img_all)
-                dist.all_reduce(ill_all)
-                ctx.set_accumulators_dev(img_all.data_ptr(), ill_all.data_ptr())
+                shotlib.reduce_context_accumulators(ctx, img_all, ill_all)
             e1.record(stream)
         torch.cuda.synchronize()
     launches = ctx.launch_count() - launches0

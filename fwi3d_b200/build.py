@@ -55,9 +55,10 @@ def _stale(target: Path, sources: list[Path]) -> bool:
 
 def build_library(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> Path:
     LIB_DIR.mkdir(exist_ok=True)
-    srcs = sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "fwi3d.h"]
+    units = sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
+    srcs = units + sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "fwi3d.h"]
     if force or ptxas_info or _stale(LIB, srcs):
-        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-shared", "-o", str(LIB), *map(str, sorted(CSRC.glob("*.cu")))]
+        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-shared", "-o", str(LIB), *map(str, units)]
         if ptxas_info:
             cmd.insert(1, "-Xptxas=-v")
         _run(cmd, verbose)

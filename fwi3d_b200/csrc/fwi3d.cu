@@ -855,10 +855,15 @@ double residual_impl(fwi_ctx *c, const float *d_obs, const float *d_cal, long lo
     return s;
 }
 
-// Host Poisson-disk sampling in a box (Bridson's method, as
-// poissonDiskSampling of src/admin/admin.cpp:138-241: 30 candidates in the
-// shell [r, 2r] around a random active point), seeded and deterministic.
-std::vector<float> poisson_points(float xm, float ym, float zm, float r, std::mt19937_64 &rng)
+// Host Poisson-disk sampling (Bridson's method, as poissonDiskSampling of
+// src/admin/admin.cpp:138-241: up to 30 candidates in the shell [r, 2r] around
+// a random active point), seeded and deterministic.  Only points outside the
+// inner box `keep_out` are kept by the random boundary (modeling.cu:571-577),
+// so candidates inside it are rejected outright and the sampling covers the
+// pad shell alone.  Conflicts are searched in the +-2 background cells
+// (cell = r/sqrt(3)) that can hold a point closer than r.
+std::vector<float> poisson_points(float xm, float ym, float zm, float r, const float keep_out[6],
+                                  std::mt19937_64 &rng)
 {
     const float cell = r / std::sqrt(3.0f);
     const int gx = std::max(1, (int)std::ceil(xm / cell)), gy = std::max(1, (int)std::ceil(ym / cell)),
@@ -867,10 +872,26 @@ std::vector<float> poisson_points(float xm, float ym, float zm, float r, std::mt
     std::vector<float> pts;  // x, y, z triples
     std::vector<int> active;
     std::uniform_real_distribution<float> U(0.0f, 1.0f);
+    // neighbour offsets whose nearest point can be closer than r
+    std::vector<int> offs;
+    for (int k = -2; k <= 2; ++k)
+        for (int j = -2; j <= 2; ++j)
+            for (int i = -2; i <= 2; ++i) {
+                auto g = [](int d) { return std::max(std::abs(d) - 1, 0); };
+                if (g(i) * g(i) + g(j) * g(j) + g(k) * g(k) < 3) {
+                    offs.push_back(i);
+                    offs.push_back(j);
+                    offs.push_back(k);
+                }
+            }
     auto cell_of = [&](float x, float y, float z, int &a, int &b, int &d) {
         a = std::min(gx - 1, (int)(x / cell));
         b = std::min(gy - 1, (int)(y / cell));
         d = std::min(gz - 1, (int)(z / cell));
+    };
+    auto inside_keep_out = [&](float x, float y, float z) {
+        return x > keep_out[0] && x < keep_out[1] && y > keep_out[2] && y < keep_out[3] && z > keep_out[4] &&
+               z < keep_out[5];
     };
     auto insert = [&](float x, float y, float z) {
         int a, b, d;
@@ -883,21 +904,23 @@ std::vector<float> poisson_points(float xm, float ym, float zm, float r, std::mt
     };
     auto valid = [&](float x, float y, float z) {
         if (x < 0 || y < 0 || z < 0 || x >= xm || y >= ym || z >= zm) return false;
+        if (inside_keep_out(x, y, z)) return false;
         int a, b, d;
         cell_of(x, y, z, a, b, d);
-        for (int k = -2; k <= 2; ++k)
-            for (int j = -2; j <= 2; ++j)
-                for (int i = -2; i <= 2; ++i) {
-                    const int A = a + j, Bq = b + k, D = d + i;
-                    if (A < 0 || Bq < 0 || D < 0 || A >= gx || Bq >= gy || D >= gz) continue;
-                    const int q = grid[D + (size_t)gz * (A + (size_t)gx * Bq)];
-                    if (q < 0) continue;
-                    const float dx = pts[3 * q] - x, dy = pts[3 * q + 1] - y, dz = pts[3 * q + 2] - z;
-                    if (dx * dx + dy * dy + dz * dz < r * r) return false;
-                }
+        for (size_t o = 0; o < offs.size(); o += 3) {
+            const int A = a + offs[o + 1], Bq = b + offs[o + 2], D = d + offs[o];
+            if (A < 0 || Bq < 0 || D < 0 || A >= gx || Bq >= gy || D >= gz) continue;
+            const int q = grid[D + (size_t)gz * (A + (size_t)gx * Bq)];
+            if (q < 0) continue;
+            const float dx = pts[3 * q] - x, dy = pts[3 * q + 1] - y, dz = pts[3 * q + 2] - z;
+            if (dx * dx + dy * dy + dz * dz < r * r) return false;
+        }
         return true;
     };
-    insert(U(rng) * xm, U(rng) * ym, U(rng) * zm);
+    for (int tries = 0; tries < 1000 && pts.empty(); ++tries) {
+        const float x = U(rng) * xm, y = U(rng) * ym, z = U(rng) * zm;
+        if (!inside_keep_out(x, y, z)) insert(x, y, z);
+    }
     const float pi = (float)M_PI;
     while (!active.empty()) {
         const int ai = (int)(U(rng) * active.size()) % (int)active.size();
@@ -1202,8 +1225,10 @@ int fwi_apply_random_boundary(fwi_ctx *c, const fwi_rbc *rbc, uint64_t seed)
             const float dh = c->g.dh;
             const float xm = (c->nxx - 1) * dh, ym = (c->nyy - 1) * dh, zm = (c->nzz - 1) * dh;
             std::mt19937_64 rng(splitmix64(seed ^ 0x5EEDB10Bull));
-            std::vector<float> pts = poisson_points(xm, ym, zm, rbc->ratio, rng);
             const float fnb = c->g.nb * dh;
+            const float keep_out[6] = {0.5f * fnb, xm - 0.5f * fnb, 0.5f * fnb, ym - 0.5f * fnb,
+                                       0.5f * fnb, zm - 0.5f * fnb};
+            std::vector<float> pts = poisson_points(xm, ym, zm, rbc->ratio, keep_out, rng);
             std::vector<Blob> blobs;
             std::uniform_real_distribution<float> U(0.0f, 1.0f);
             for (size_t q = 0; q < pts.size() / 3; ++q) {
@@ -1359,6 +1384,16 @@ int fwi_reset_accumulators(fwi_ctx *c)
         CK(cudaMemsetAsync(c->acc_ill.p, 0, bytes, c->stream));
         CK(cudaStreamSynchronize(c->stream));
         c->acc_dirty = false;
+    });
+}
+
+int fwi_zero_image(fwi_ctx *c)
+{
+    if (!c) return FWI_ERR_ARG;
+    return guarded(c, [&] {
+        ensure_fields(c, true);
+        CK(cudaMemsetAsync(c->acc_img.p, 0, (size_t)c->B * c->vol * sizeof(float), c->stream));
+        CK(cudaStreamSynchronize(c->stream));
     });
 }
 

@@ -56,6 +56,7 @@ SIGNATURES = {
     "fwi_rtm_shots": (_i, [_p, _ip, _i, _fp]),
     "fwi_rtm_shots_dev": (_i, [_p, _ip, _i, _p]),
     "fwi_reset_accumulators": (_i, [_p]),
+    "fwi_zero_image": (_i, [_p]),
     "fwi_get_accumulators": (_i, [_p, _fp, _fp]),
     "fwi_get_accumulators_dev": (_i, [_p, _p, _p]),
     "fwi_set_accumulators_dev": (_i, [_p, _p, _p]),
@@ -67,6 +68,10 @@ SIGNATURES = {
     "fwi_residual_dev": (_i, [_p, _p, _p, _i64, _p, _dp]),
     "fwi_residual_noalloc": (_i, [_p, _p, _i64, _p, _p, _p]),
     "fwi_dot_dev": (_i, [_p, _p, _p, _i64, _dp]),
+    "fwi_catch_parameter": (_i, [C.c_char_p, C.c_char_p, C.c_char_p, _i]),
+    "fwi_read_points": (_i, [C.c_char_p, _fp, _fp, _fp, _i, _ip]),
+    "fwi_read_binary": (_i, [C.c_char_p, _fp, _i64]),
+    "fwi_write_binary": (_i, [C.c_char_p, _fp, _i64]),
     "fwi_last_timing": (_i, [_p, _fp, _fp]),
     "fwi_launch_count": (_i, [_p, C.POINTER(C.c_int64)]),
     "fwi_get_tiles": (_i, [_p, _ip, _ip]),
@@ -282,6 +287,9 @@ class Context:
     def reset_accumulators(self):
         self._check(self.lib.fwi_reset_accumulators(self.h))
 
+    def zero_image(self):
+        self._check(self.lib.fwi_zero_image(self.h))
+
     def get_accumulators(self):
         img = np.empty(self.padded_shape, np.float32)
         ill = np.empty(self.padded_shape, np.float32)
@@ -347,6 +355,29 @@ class Context:
 
     def set_tiles(self, fwd: int, bwd: int):
         self._check(self.lib.fwi_set_tiles(self.h, fwd, bwd))
+
+
+def catch_parameter(file, key: str) -> str:
+    """The reference's parameters.txt lookup (prefix match, '#' comments)."""
+    buf = C.create_string_buffer(4096)
+    st = load().fwi_catch_parameter(str(file).encode(), key.encode(), buf, 4096)
+    if st != FWI_OK:
+        raise FwiError(st, f"cannot read {file}")
+    return buf.value.decode()
+
+
+def read_points(file) -> np.ndarray:
+    """SPS/RPS file -> (n, 3) float32 x, y, z."""
+    lib = load()
+    n = C.c_int()
+    st = lib.fwi_read_points(str(file).encode(), None, None, None, 0, C.byref(n))
+    if st != FWI_OK:
+        raise FwiError(st, f"cannot read {file}")
+    cols = [np.zeros(n.value, np.float32) for _ in range(3)]
+    st = lib.fwi_read_points(str(file).encode(), *[_fptr(c) for c in cols], n.value, C.byref(n))
+    if st != FWI_OK:
+        raise FwiError(st, f"malformed {file}")
+    return np.stack(cols, axis=1)
 
 
 NOALLOC_MAX_N = 268435456

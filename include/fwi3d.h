@@ -140,6 +140,10 @@ int fwi_rtm_shots(fwi_ctx *ctx, const int *shots, int nshots, const float *data)
 int fwi_rtm_shots_dev(fwi_ctx *ctx, const int *shots, int nshots, const float *d_data);
 /* Zero the padded image / gradient and illumination accumulators. */
 int fwi_reset_accumulators(fwi_ctx *ctx);
+/* Zero only the image / gradient accumulator and keep the illumination: the
+ * reference zeroes its gradient for every gradient (inversion.cu:210) but never
+ * its illumination (d_sumPs_rbc, inversion.cu:142). */
+int fwi_zero_image(fwi_ctx *ctx);
 /* Raw padded accumulators [nzz,nxx,nyy] (either pointer may be NULL). */
 int fwi_get_accumulators(fwi_ctx *ctx, float *image_padded, float *illum_padded);
 /* Same, into caller device buffers [nzz,nxx,nyy] (for a cross-GPU sum of
@@ -184,6 +188,18 @@ int fwi_residual_noalloc(const float *d_obs, const float *d_cal, int64_t n, floa
                          double *d_sum_sq, void *stream);
 /* FP64 dot product of two device vectors (gradient dot products). */
 int fwi_dot_dev(fwi_ctx *ctx, const float *d_a, const float *d_b, int64_t n, double *out);
+
+/* ---- reference file formats (host only, no device needed) --------------- */
+/* catch_parameter (src/admin/admin.cpp:86-121): value of the first line that
+ * starts with `key` and not with '#' or ' ' -- a prefix match -- taken from two
+ * characters after '=' up to '#', spaces removed.  Missing key: empty value. */
+int fwi_catch_parameter(const char *parameters_file, const char *key, char *value, int cap);
+/* SPS/RPS "x,y,z" lines in metres, '#' lines skipped (src/geometry/geometry.cpp:
+ * 3-47).  x == NULL returns only the count in *n. */
+int fwi_read_points(const char *file, float *x, float *y, float *z, int cap, int *n);
+/* Raw float32 files (import/export_binary_float, src/admin/admin.cpp:46-70). */
+int fwi_read_binary(const char *file, float *buf, int64_t n);
+int fwi_write_binary(const char *file, const float *buf, int64_t n);
 
 /* ---- diagnostics ------------------------------------------------------- */
 /* Device time [ms] of the last call's forward and backward time loops. */
