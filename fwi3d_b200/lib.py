@@ -68,6 +68,14 @@ SIGNATURES = {
     "fwi_residual_dev": (_i, [_p, _p, _p, _i64, _p, _dp]),
     "fwi_residual_noalloc": (_i, [_p, _p, _i64, _p, _p, _p]),
     "fwi_dot_dev": (_i, [_p, _p, _p, _i64, _dp]),
+    "fwi_cnn_create": (_i, [C.c_uint64, C.POINTER(_p)]),
+    "fwi_cnn_destroy": (_i, [_p]),
+    "fwi_cnn_last_error": (_i, [_p, C.c_char_p, _i]),
+    "fwi_cnn_set_stream": (_i, [_p, _p]),
+    "fwi_cnn_get_weights": (_i, [_p, _fp, _fp]),
+    "fwi_cnn_set_weights": (_i, [_p, _fp, _fp]),
+    "fwi_cnn_forward": (_i, [_p, _i, _i, _i, _p, _p]),
+    "fwi_cnn_train_step": (_i, [_p, _i, _i, _i, _p, _p, _f, _dp, _fp, _fp]),
     "fwi_catch_parameter": (_i, [C.c_char_p, C.c_char_p, C.c_char_p, _i]),
     "fwi_read_points": (_i, [C.c_char_p, _fp, _fp, _fp, _i, _ip]),
     "fwi_read_binary": (_i, [C.c_char_p, _fp, _i64]),
@@ -355,6 +363,68 @@ class Context:
 
     def set_tiles(self, fwd: int, bwd: int):
         self._check(self.lib.fwi_set_tiles(self.h, fwd, bwd))
+
+
+class Cnn:
+    """The learned preconditioner network (fwi_cnn_*): BF16 tensor-core
+    forward/backward, FP32 Adam.  Volumes are device pointers."""
+
+    NL, TAPS, CH = 4, 27, 16
+
+    def __init__(self, seed=0):
+        self.lib = load()
+        h = C.c_void_p()
+        st = self.lib.fwi_cnn_create(C.c_uint64(seed), C.byref(h))
+        if st != FWI_OK:
+            raise FwiError(st, "fwi_cnn_create")
+        self.h = h
+
+    def _check(self, st):
+        if st != FWI_OK:
+            buf = C.create_string_buffer(512)
+            self.lib.fwi_cnn_last_error(self.h, buf, 512)
+            raise FwiError(st, buf.value.decode(errors="replace"))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.fwi_cnn_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int):
+        self._check(self.lib.fwi_cnn_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def get_weights(self):
+        w = np.zeros((self.NL, self.TAPS, self.CH, self.CH), np.float32)
+        b = np.zeros((self.NL, self.CH), np.float32)
+        self._check(self.lib.fwi_cnn_get_weights(self.h, _fptr(w), _fptr(b)))
+        return w, b
+
+    def set_weights(self, w, b):
+        w = np.ascontiguousarray(w, np.float32)
+        b = np.ascontiguousarray(b, np.float32)
+        self._check(self.lib.fwi_cnn_set_weights(self.h, _fptr(w), _fptr(b)))
+
+    def forward(self, shape_zxy, d_in: int, d_out: int):
+        nz, nx, ny = shape_zxy
+        self._check(self.lib.fwi_cnn_forward(self.h, nz, nx, ny, C.c_void_p(d_in), C.c_void_p(d_out)))
+
+    def train_step(self, shape_zxy, d_in: int, d_target: int, lr: float, want_grads=False):
+        nz, nx, ny = shape_zxy
+        loss = C.c_double()
+        gw = gb = None
+        if want_grads:
+            gw = np.zeros((self.NL, self.TAPS, self.CH, self.CH), np.float32)
+            gb = np.zeros((self.NL, self.CH), np.float32)
+        self._check(self.lib.fwi_cnn_train_step(self.h, nz, nx, ny, C.c_void_p(d_in), C.c_void_p(d_target), lr,
+                                                C.byref(loss), _fptr(gw) if gw is not None else None,
+                                                _fptr(gb) if gb is not None else None))
+        return (loss.value, gw, gb) if want_grads else loss.value
 
 
 def catch_parameter(file, key: str) -> str:

@@ -189,6 +189,26 @@ int fwi_residual_noalloc(const float *d_obs, const float *d_cal, int64_t n, floa
 /* FP64 dot product of two device vectors (gradient dot products). */
 int fwi_dot_dev(fwi_ctx *ctx, const float *d_a, const float *d_b, int64_t n, double *out);
 
+/* ---- learned preconditioner (no counterpart in the reference) ----------- */
+/* A 4-layer 3-D CNN, 3 -> 16 -> 16 -> 16 -> 1 channels, 3^3 kernels, ReLU,
+ * BF16 tensor-core forward/backward with FP32 accumulation and FP32 Adam.
+ * Inputs are three normalised FP32 device volumes [3][nz*nx*ny] (raw
+ * gradient, velocity, illumination); the output is one FP32 device volume
+ * (the predicted model update).  Weights: [4][27][16 co][16 ci] FP32,
+ * tap t = (dz+1) + 3(dx+1) + 9(dy+1); biases [4][16]. */
+typedef struct fwi_cnn fwi_cnn;
+int fwi_cnn_create(uint64_t seed, fwi_cnn **out);
+int fwi_cnn_destroy(fwi_cnn *cnn);
+int fwi_cnn_last_error(fwi_cnn *cnn, char *buf, int cap);
+int fwi_cnn_set_stream(fwi_cnn *cnn, void *stream);
+int fwi_cnn_get_weights(fwi_cnn *cnn, float *weights, float *biases);
+int fwi_cnn_set_weights(fwi_cnn *cnn, const float *weights, const float *biases);
+int fwi_cnn_forward(fwi_cnn *cnn, int nz, int nx, int ny, const float *d_in, float *d_out);
+/* Loss 0.5 mean (f(x) - target)^2; its weight/bias gradients (host, may be
+ * NULL); an Adam step with learning rate lr when lr > 0. */
+int fwi_cnn_train_step(fwi_cnn *cnn, int nz, int nx, int ny, const float *d_in, const float *d_target, float lr,
+                       double *loss, float *grad_w, float *grad_b);
+
 /* ---- reference file formats (host only, no device needed) --------------- */
 /* catch_parameter (src/admin/admin.cpp:86-121): value of the first line that
  * starts with `key` and not with '#' or ' ' -- a prefix match -- taken from two
