@@ -79,6 +79,7 @@ class Workload:
     start: np.ndarray | None = None
     rbc: dict = field(default_factory=dict)
     abc_factor: float = 0.004
+    zmask: float = 0.0  # depth_mask [m]: gradient muted above it (acquisition imprint)
 
 
 def modeling_101(nt=1001):
@@ -135,7 +136,8 @@ def gradient_401(nt=2501, seed=3):
     src = surface_grid(xs, xs, 12.5)
     rec = surface_grid(np.arange(0, (nx - 1) * dh + 1e-3, 25.0), np.arange(0, (ny - 1) * dh + 1e-3, 25.0), 12.5)
     return Workload("gradient-401x401x201", nz, nx, ny, dh, nt, 1e-3, 30.0, 41, v, src, rec,
-                    start=smooth_slowness(v, 200.0, dh), rbc=dict(kind=0, ratio=100.0, varVp=1000.0))
+                    start=smooth_slowness(v, 200.0, dh), rbc=dict(kind=0, ratio=100.0, varVp=1000.0),
+                    zmask=100.0)
 
 
 def cnn_128(index, nt=1201):
@@ -154,7 +156,8 @@ def cnn_128(index, nt=1201):
     src = surface_grid(xs, xs, 10.0)
     rec = surface_grid(np.arange(0, (n - 1) * dh + 1e-3, 20.0), np.arange(0, (n - 1) * dh + 1e-3, 20.0), 10.0)
     return Workload(f"cnn-128^3-{index}", n, n, n, dh, nt, 1e-3, 30.0, 50, v, src, rec,
-                    start=smooth_slowness(v, 150.0, dh), rbc=dict(kind=0, ratio=100.0, varVp=1000.0))
+                    start=smooth_slowness(v, 150.0, dh), rbc=dict(kind=0, ratio=100.0, varVp=1000.0),
+                    zmask=60.0)
 
 
 def fwi_301(nt=2001):
@@ -169,7 +172,8 @@ def fwi_301(nt=2001):
     src = surface_grid(xs, xs, 10.0)
     rec = surface_grid(np.arange(0, (nx - 1) * dh + 1e-3, 20.0), np.arange(0, (ny - 1) * dh + 1e-3, 20.0), 10.0)
     return Workload("fwi-301x301x151", nz, nx, ny, dh, nt, 1e-3, 24.0, 50, v, src, rec,
-                    start=smooth_slowness(v, 200.0, dh), rbc=dict(kind=0, ratio=100.0, varVp=1000.0))
+                    start=smooth_slowness(v, 200.0, dh), rbc=dict(kind=0, ratio=100.0, varVp=1000.0),
+                    zmask=80.0)
 
 
 def small_case(n=40, nb=8, nt=120, seed=0, dh=10.0, nrec_side=5):
@@ -182,3 +186,23 @@ def small_case(n=40, nb=8, nt=120, seed=0, dh=10.0, nrec_side=5):
     xs = np.linspace(2 * dh, (n + 1) * dh, nrec_side)
     rec = surface_grid(xs, np.linspace(2 * dh, n * dh, nrec_side), 3 * dh)
     return Workload(f"small-{n}", n, n + 4, n + 2, dh, nt, 1e-3, 60.0, nb, v, src, rec)
+
+
+def small_fwi(index, n=48, nt=400):
+    """Small inversion problem `index` for tests: n^3 at 10 m, three layers with
+    one or two Gaussian anomalies of +-15 % (sigma 50-90 m), start model
+    smoothed with sigma 80 m, 2 x 2 shots, receivers every 20 m, 10 Hz peak."""
+    rng = np.random.default_rng(5000 + index)
+    dh = 10.0
+    vels = np.sort(rng.uniform(1600, 3000, 3))
+    tops = [0.0, *np.sort(rng.uniform(0.25, 0.75, 2)) * n * dh]
+    v = layered(n, n, n, dh, vels, tops)
+    for _ in range(rng.integers(1, 3)):
+        c = rng.uniform(0.3, 0.7, 3) * (n - 1) * dh
+        v = add_gaussian(v, dh, c, rng.uniform(50, 90), rng.choice([-0.15, 0.15]))
+    xs = (np.arange(2) + 0.5) * (n - 1) * dh / 2
+    src = surface_grid(xs, xs, 10.0)
+    g = np.arange(0, (n - 1) * dh + 1e-3, 20.0)
+    rec = surface_grid(g, g, 10.0)
+    return Workload(f"small-fwi-{index}", n, n, n, dh, nt, 1e-3, 30.0, 20, v, src, rec,
+                    start=smooth_slowness(v, 80.0, dh), rbc=dict(kind=0, ratio=40.0, varVp=400.0), zmask=40.0)
