@@ -112,14 +112,13 @@ __global__ void __launch_bounds__(WARPS * 32)
         }
         const long long base = ((long long)k * g.nx + j) * g.nz;
         const int za = z0 + grp, zb = za + 8;
-        if (MODE == 2) {
+        if constexpr (MODE == 2) {
             // last layer: only output channel 0 is real (thread q == 0 of n-tile 0)
             if (q == 0) {
                 if (za < g.nz) out32[base + za] = acc0[0] + bias[0];
                 if (zb < g.nz) out32[base + zb] = acc0[2] + bias[0];
             }
-            continue;
-        }
+        } else {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int z = h ? zb : za;
@@ -140,6 +139,7 @@ __global__ void __launch_bounds__(WARPS * 32)
                 }
                 *reinterpret_cast<uint32_t *>(out + v * CH + co) = pack_bf16(x0, x1);
             }
+        }
         }
     }
 }

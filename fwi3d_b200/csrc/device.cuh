@@ -125,8 +125,8 @@ __device__ __forceinline__ uint64_t global_ns()
     return t;
 }
 
-// Wait for phase `parity` of an mbarrier, giving up after kWaitLimitNs.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+// Wait for phase `parity` of an mbarrier, giving up after limit_ns.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint64_t limit_ns = kWaitLimitNs)
 {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = global_ns();
@@ -134,7 +134,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
 #pragma unroll 1
         for (int i = 0; i < 32; ++i)
             if (mbar_try_wait(bar, parity)) return true;
-        if (global_ns() - t0 > kWaitLimitNs) return false;
+        if (global_ns() - t0 > limit_ns) return false;
     }
 }
 

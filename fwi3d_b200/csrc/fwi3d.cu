@@ -1540,6 +1540,17 @@ int fwi_dot_dev(fwi_ctx *c, const float *a, const float *b, int64_t n, double *o
     });
 }
 
+int fwi_selftest_bounded_wait(fwi_ctx *c, int limit_ms)
+{
+    if (!c || limit_ms < 1 || limit_ms > 2000) return FWI_ERR_ARG;
+    return guarded(c, [&] {
+        bounded_wait_probe_kernel<<<1, 32, 0, c->stream>>>((uint64_t)limit_ms * 1000000ull);
+        CK(cudaGetLastError());
+        ++c->launches;
+        check_status(c);
+    });
+}
+
 int fwi_last_timing(fwi_ctx *c, float *fwd_ms, float *bwd_ms)
 {
     if (!c) return FWI_ERR_ARG;

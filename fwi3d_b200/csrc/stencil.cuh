@@ -98,6 +98,20 @@ __device__ __forceinline__ void raise_status(unsigned bits) { atomicOr(&g_status
 // completing ends after one bounded wait instead of one per step.
 __device__ __forceinline__ bool status_failed() { return *(volatile unsigned int *)&g_status != 0; }
 
+// Exercises the bounded-wait path without any fault: an mbarrier that expects
+// two arrivals gets one, so its phase never completes; the wait gives up after
+// limit_ns and reports through g_status exactly like the stencil kernels.
+__global__ void bounded_wait_probe_kernel(uint64_t limit_ns)
+{
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 2);
+        fence_mbar_init();
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&bar)) : "memory");
+        if (!mbar_wait(&bar, 0, limit_ns)) raise_status(kErrTimeout);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Forward leapfrog step.
 //   mh: halo-box map over A (the field read with the stencil)

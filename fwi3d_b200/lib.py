@@ -17,7 +17,8 @@ from pathlib import Path
 
 import numpy as np
 
-LIB_PATH = Path(__file__).resolve().parent / "lib" / "libfwi3d.so"
+# FWI3D_LIB selects another build of the library (e.g. a tuning variant).
+LIB_PATH = Path(os.environ.get("FWI3D_LIB", Path(__file__).resolve().parent / "lib" / "libfwi3d.so"))
 
 FWI_OK = 0
 BOUNDARY_ABC = 0
@@ -80,6 +81,7 @@ SIGNATURES = {
     "fwi_read_points": (_i, [C.c_char_p, _fp, _fp, _fp, _i, _ip]),
     "fwi_read_binary": (_i, [C.c_char_p, _fp, _i64]),
     "fwi_write_binary": (_i, [C.c_char_p, _fp, _i64]),
+    "fwi_selftest_bounded_wait": (_i, [_p, _i]),
     "fwi_last_timing": (_i, [_p, _fp, _fp]),
     "fwi_launch_count": (_i, [_p, C.POINTER(C.c_int64)]),
     "fwi_get_tiles": (_i, [_p, _ip, _ip]),

@@ -222,6 +222,10 @@ int fwi_read_binary(const char *file, float *buf, int64_t n);
 int fwi_write_binary(const char *file, const float *buf, int64_t n);
 
 /* ---- diagnostics ------------------------------------------------------- */
+/* Runs one wait that nothing completes, bounded by limit_ms (1..2000): the
+ * kernels' timeout path end to end.  Returns FWI_ERR_TIMEOUT and leaves the
+ * context usable. */
+int fwi_selftest_bounded_wait(fwi_ctx *ctx, int limit_ms);
 /* Device time [ms] of the last call's forward and backward time loops. */
 int fwi_last_timing(fwi_ctx *ctx, float *fwd_ms, float *bwd_ms);
 /* Kernel launches issued by the library since creation (graph nodes count

@@ -182,3 +182,14 @@ def test_cfl_violation_is_reported():
     with pytest.raises(lib.FwiError) as e:
         ctx.set_velocity(np.full(w.vp.shape, 9000.0, np.float32))
     assert e.value.code == 7
+
+
+def test_bounded_wait_reports_a_timeout_and_the_context_survives():
+    """A wait on an mbarrier that nothing completes gives up after its limit
+    and surfaces as FWI_ERR_TIMEOUT; the next call works normally."""
+    w = synth.small_case(n=20, nb=4, nt=40)
+    ctx = context(w, lib.BOUNDARY_RBC)
+    assert ctx.lib.fwi_selftest_bounded_wait(ctx.h, 50) == 4
+    ctx.set_velocity(w.vp)
+    seis = ctx.model_shots([0])[0]
+    assert np.all(np.isfinite(seis)) and np.abs(seis).max() > 0
