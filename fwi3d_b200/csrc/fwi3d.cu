@@ -33,7 +33,7 @@ namespace {
 constexpr int kNumTiles = 10;
 constexpr int kTileTZ4[kNumTiles] = {16, 16, 32, 24, 25, 37, 19, 8, 32, 49};
 constexpr int kTileTX[kNumTiles] = {8, 16, 8, 8, 8, 8, 8, 16, 4, 4};
-constexpr int SHF = 7, SCF = 3;  // forward rings: halo slots, centre slots
+constexpr int SHF = 8, SCF = 3;  // forward rings: halo slots, centre slots
 constexpr int SHB = 7, SCB = 3;  // backward rings
 
 template <int I>
