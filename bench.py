@@ -133,12 +133,14 @@ def max_over_ranks(x: float, ws: int) -> float:
     return float(t.item())
 
 
-def workload(name):
+def workload(name, nt=None):
+    """The benchmark workloads; nt shortens the time axis (profiling runs only)."""
     from fwi3d_b200 import synth
+    kw = {} if nt is None else {"nt": nt}
     if name == "rtm":
-        return synth.rtm_201()
+        return synth.rtm_201(**kw)
     if name == "modeling":
-        return synth.modeling_101()
+        return synth.modeling_101(**kw)
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -171,7 +173,7 @@ def run_ours(args, ws, rank, local):
     import torch
     from fwi3d_b200 import lib
 
-    w = workload(args.workload)
+    w = workload(args.workload, args.nt)
     rtm = args.workload == "rtm"
     boundary = lib.BOUNDARY_RBC
     ctx = lib.Context(w.nz, w.nx, w.ny, w.nb, w.dh, w.nt, w.dt, w.fmax, boundary, w.abc_factor, 1, 0)
@@ -400,6 +402,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
     ap.add_argument("--tiles", default="", help="fixed forward,backward tile indices instead of autotuning")
+    ap.add_argument("--nt", type=int, default=None, help="shorter time axis for profiling runs (not a bench number)")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     if args.impl == "reference":
