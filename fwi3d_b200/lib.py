@@ -77,6 +77,7 @@ SIGNATURES = {
     "fwi_cnn_set_weights": (_i, [_p, _fp, _fp]),
     "fwi_cnn_forward": (_i, [_p, _i, _i, _i, _p, _p]),
     "fwi_cnn_train_step": (_i, [_p, _i, _i, _i, _p, _p, _f, _dp, _fp, _fp]),
+    "fwi_prepare_rtm_input": (_i, [_fp, _fp, _i, _i, _fp, _fp, _f, _f, _f, _f, _f, _f]),
     "fwi_catch_parameter": (_i, [C.c_char_p, C.c_char_p, C.c_char_p, _i]),
     "fwi_read_points": (_i, [C.c_char_p, _fp, _fp, _fp, _i, _ip]),
     "fwi_read_binary": (_i, [C.c_char_p, _fp, _i64]),
@@ -427,6 +428,20 @@ class Cnn:
                                                 C.byref(loss), _fptr(gw) if gw is not None else None,
                                                 _fptr(gb) if gb is not None else None))
         return (loss.value, gw, gb) if want_grads else loss.value
+
+
+def prepare_rtm_input(seis, rec_xy, src_xy, dt, velocity=3600.0, time_delay=0.18, gstd=30.0):
+    """RTM input gather of one shot (fwi_prepare_rtm_input): seis (nrec, nt)."""
+    a = np.ascontiguousarray(seis, np.float32)
+    nrec, nt = a.shape
+    rx = np.ascontiguousarray(np.asarray(rec_xy)[:, 0], np.float32)
+    ry = np.ascontiguousarray(np.asarray(rec_xy)[:, 1], np.float32)
+    out = np.empty_like(a)
+    st = load().fwi_prepare_rtm_input(_fptr(a), _fptr(out), nt, nrec, _fptr(rx), _fptr(ry), float(src_xy[0]),
+                                      float(src_xy[1]), velocity, time_delay, dt, gstd)
+    if st != FWI_OK:
+        raise FwiError(st, "fwi_prepare_rtm_input")
+    return out
 
 
 def catch_parameter(file, key: str) -> str:

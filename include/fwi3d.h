@@ -209,6 +209,15 @@ int fwi_cnn_forward(fwi_cnn *cnn, int nz, int nx, int ny, const float *d_in, flo
 int fwi_cnn_train_step(fwi_cnn *cnn, int nz, int nx, int ny, const float *d_in, const float *d_target, float lr,
                        double *loss, float *grad_w, float *grad_b);
 
+/* ---- pipeline preprocessing -------------------------------------------- */
+/* RTM input data of one shot (run/generate_input_data.py:28-46): scale the
+ * Fortran [nt, nrec] gather by 1/max|d|, then taper each trace before its
+ * direct-wave sample int((|x_r - x_s|/velocity + time_delay)/dt) with
+ * exp(-0.5 ((t - t_r)/gstd)^2).  Host buffers; the reference script uses
+ * velocity 3600 m/s, time_delay 0.18 s, gstd 30 samples. */
+int fwi_prepare_rtm_input(const float *seis, float *out, int nt, int nrec, const float *rx, const float *ry,
+                          float sx, float sy, float velocity, float time_delay, float dt, float gstd);
+
 /* ---- reference file formats (host only, no device needed) --------------- */
 /* catch_parameter (src/admin/admin.cpp:86-121): value of the first line that
  * starts with `key` and not with '#' or ' ' -- a prefix match -- taken from two
