@@ -12,6 +12,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <future>
 #include <map>
 #include <random>
 #include <string>
@@ -206,6 +207,23 @@ struct Graph {
     int generation = -1;
 };
 
+struct BlobKey {
+    uint64_t seed = 0;
+    float xm = 0, ym = 0, zm = 0, ratio = 0, varVp = 0, fnb = 0;
+    bool operator==(const BlobKey &o) const
+    {
+        return seed == o.seed && xm == o.xm && ym == o.ym && zm == o.zm && ratio == o.ratio && varVp == o.varVp &&
+               fnb == o.fnb;
+    }
+};
+
+struct BlobSet {
+    std::vector<Blob> blobs;
+    std::vector<int> first, list;
+    int nbz = 0, nbx = 0, nby = 0;
+    float bin = 0;
+};
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -242,6 +260,12 @@ struct fwi_ctx {
     DevBuf<double> partial, dsum;
     DevBuf<unsigned int> ubits;
     DevBuf<float> post;  // [nz*nx*ny] post-processing output
+    DevBuf<float> stage;  // host-model uploads and padded downloads
+    DevBuf<Blob> blob_dev;
+    DevBuf<int> bin_first, bin_list;
+    BlobSet blobs_now;               // host copy behind the last blob upload
+    std::future<BlobSet> blobs_next; // blob set of the next seed, built on a host thread
+    BlobKey blobs_next_key;
     int generation = 0;  // bumped whenever a buffer a graph points at moves
     bool acc_dirty = false;
 
@@ -944,6 +968,54 @@ std::vector<float> poisson_points(float xm, float ym, float zm, float r, const f
     return pts;
 }
 
+// The Gaussian blobs of one random boundary (random_boundary_gp,
+// src/modeling/modeling.cu:566-591): Poisson-disk centres outside the inner
+// half-pad box, radius U(0.2 r, r), amplitude U(0.5 varVp, varVp), negative with
+// probability 1/3, binned for the blob kernel.  A pure function of its
+// arguments, so it can run on a host thread while the GPU works.
+BlobSet make_blobs(BlobKey k)
+{
+    BlobSet out;
+    std::mt19937_64 rng(splitmix64(k.seed ^ 0x5EEDB10Bull));
+    const float h = 0.5f * k.fnb;
+    const float keep_out[6] = {h, k.xm - h, h, k.ym - h, h, k.zm - h};
+    std::vector<float> pts = poisson_points(k.xm, k.ym, k.zm, k.ratio, keep_out, rng);
+    std::uniform_real_distribution<float> U(0.0f, 1.0f);
+    for (size_t q = 0; q < pts.size() / 3; ++q) {
+        const float x = pts[3 * q], y = pts[3 * q + 1], z = pts[3 * q + 2];
+        if (x > h && x < k.xm - h && y > h && y < k.ym - h && z > h && z < k.zm - h) continue;
+        Blob b;
+        b.x = x;
+        b.y = y;
+        b.z = z;
+        b.r = k.ratio * (0.2f + 0.8f * U(rng));
+        const float A = k.varVp * (0.5f + 0.5f * U(rng));
+        b.amp = ((rng() % 3) == 0 ? -1.0f : 1.0f) * A;
+        out.blobs.push_back(b);
+    }
+    out.bin = 5.0f * k.ratio;
+    out.nbz = (int)(k.zm / out.bin) + 1;
+    out.nbx = (int)(k.xm / out.bin) + 1;
+    out.nby = (int)(k.ym / out.bin) + 1;
+    std::vector<std::vector<int>> bins((size_t)out.nbz * out.nbx * out.nby);
+    for (size_t q = 0; q < out.blobs.size(); ++q) {
+        const Blob &b = out.blobs[q];
+        const float e = 5.0f * b.r;
+        auto lo = [&](float v, int n) { return std::max(0, std::min(n - 1, (int)std::floor((v - e) / out.bin))); };
+        auto hi = [&](float v, int n) { return std::max(0, std::min(n - 1, (int)std::floor((v + e) / out.bin))); };
+        for (int by = lo(b.y, out.nby); by <= hi(b.y, out.nby); ++by)
+            for (int bx = lo(b.x, out.nbx); bx <= hi(b.x, out.nbx); ++bx)
+                for (int bz = lo(b.z, out.nbz); bz <= hi(b.z, out.nbz); ++bz)
+                    bins[bz + (size_t)out.nbz * (bx + (size_t)out.nbx * by)].push_back((int)q);
+    }
+    out.first.assign(1, 0);
+    for (auto &v : bins) {
+        out.list.insert(out.list.end(), v.begin(), v.end());
+        out.first.push_back((int)out.list.size());
+    }
+    return out;
+}
+
 float device_max_abs(fwi_ctx *c, const float *v)
 {
     c->ubits.ensure(1);
@@ -1089,6 +1161,11 @@ int fwi_destroy(fwi_ctx *c)
     c->dsum.release();
     c->ubits.release();
     c->post.release();
+    c->stage.release();
+    c->blob_dev.release();
+    c->bin_first.release();
+    c->bin_list.release();
+    if (c->blobs_next.valid()) c->blobs_next.wait();
     for (auto &e : c->ev)
         if (e) cudaEventDestroy(e);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -1131,19 +1208,13 @@ int fwi_set_velocity(fwi_ctx *c, const float *vp)
         }
         c->vmin = lo;
         c->vmax = hi;
-        float *d_in = nullptr;
-        CK(cudaMalloc((void **)&d_in, n * sizeof(float)));
-        cudaError_t e = cudaMemcpyAsync(d_in, vp, n * sizeof(float), cudaMemcpyHostToDevice, c->stream);
-        if (e == cudaSuccess) {
-            pad_edges_kernel<<<grid_blocks(c->vol), 256, 0, c->stream>>>(d_in, c->g.nz, c->g.nx, c->g.ny, c->g.nb,
-                                                                         c->nzz, c->nxx, c->nyy, c->ldz, c->vp.p);
-            e = cudaGetLastError();
-        }
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(c->vp_clean.p, c->vp.p, c->vol * sizeof(float), cudaMemcpyDeviceToDevice, c->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-        cudaFree(d_in);
-        CK(e);
+        c->stage.ensure(n);
+        CK(cudaMemcpyAsync(c->stage.p, vp, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+        pad_edges_kernel<<<grid_blocks(c->vol), 256, 0, c->stream>>>(c->stage.p, c->g.nz, c->g.nx, c->g.ny, c->g.nb,
+                                                                     c->nzz, c->nxx, c->nyy, c->ldz, c->vp.p);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(c->vp_clean.p, c->vp.p, c->vol * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
         c->launches += 1;
         check_cfl(c);
         c->have_vp = true;
@@ -1163,19 +1234,13 @@ int fwi_set_padded_velocity(fwi_ctx *c, const float *vpp)
         }
         c->vmin = lo;
         c->vmax = hi;
-        float *d_in = nullptr;
-        CK(cudaMalloc((void **)&d_in, n * sizeof(float)));
-        cudaError_t e = cudaMemcpyAsync(d_in, vpp, n * sizeof(float), cudaMemcpyHostToDevice, c->stream);
-        if (e == cudaSuccess) {
-            dense_to_pitched_kernel<<<grid_blocks(c->vol), 256, 0, c->stream>>>(d_in, c->nzz, c->nxx, c->nyy, c->ldz,
-                                                                                c->vp.p);
-            e = cudaGetLastError();
-        }
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(c->vp_clean.p, c->vp.p, c->vol * sizeof(float), cudaMemcpyDeviceToDevice, c->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-        cudaFree(d_in);
-        CK(e);
+        c->stage.ensure(n);
+        CK(cudaMemcpyAsync(c->stage.p, vpp, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+        dense_to_pitched_kernel<<<grid_blocks(c->vol), 256, 0, c->stream>>>(c->stage.p, c->nzz, c->nxx, c->nyy,
+                                                                            c->ldz, c->vp.p);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(c->vp_clean.p, c->vp.p, c->vol * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
         c->launches += 1;
         check_cfl(c);
         c->have_vp = true;
@@ -1187,14 +1252,12 @@ int fwi_get_padded_velocity(fwi_ctx *c, float *vpp)
     if (!c || !vpp) return FWI_ERR_ARG;
     return guarded(c, [&] {
         const size_t n = (size_t)c->nzz * c->nxx * c->nyy;
-        float *d_out = nullptr;
-        CK(cudaMalloc((void **)&d_out, n * sizeof(float)));
-        pitched_to_dense_kernel<<<grid_blocks(n), 256, 0, c->stream>>>(c->vp.p, c->nzz, c->nxx, c->nyy, c->ldz, d_out);
-        cudaError_t e = cudaGetLastError();
-        if (e == cudaSuccess) e = cudaMemcpyAsync(vpp, d_out, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-        cudaFree(d_out);
-        CK(e);
+        c->stage.ensure(n);
+        pitched_to_dense_kernel<<<grid_blocks(n), 256, 0, c->stream>>>(c->vp.p, c->nzz, c->nxx, c->nyy, c->ldz,
+                                                                       c->stage.p);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(vpp, c->stage.p, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
         c->launches += 1;
     });
 }
@@ -1223,69 +1286,47 @@ int fwi_apply_random_boundary(fwi_ctx *c, const fwi_rbc *rbc, uint64_t seed)
         c->launches += 1;
         if (rbc->kind == 0 && rbc->ratio > 0 && rbc->varVp > 0) {
             const float dh = c->g.dh;
-            const float xm = (c->nxx - 1) * dh, ym = (c->nyy - 1) * dh, zm = (c->nzz - 1) * dh;
-            std::mt19937_64 rng(splitmix64(seed ^ 0x5EEDB10Bull));
-            const float fnb = c->g.nb * dh;
-            const float keep_out[6] = {0.5f * fnb, xm - 0.5f * fnb, 0.5f * fnb, ym - 0.5f * fnb,
-                                       0.5f * fnb, zm - 0.5f * fnb};
-            std::vector<float> pts = poisson_points(xm, ym, zm, rbc->ratio, keep_out, rng);
-            std::vector<Blob> blobs;
-            std::uniform_real_distribution<float> U(0.0f, 1.0f);
-            for (size_t q = 0; q < pts.size() / 3; ++q) {
-                const float x = pts[3 * q], y = pts[3 * q + 1], z = pts[3 * q + 2];
-                if (x > 0.5f * fnb && x < xm - 0.5f * fnb && y > 0.5f * fnb && y < ym - 0.5f * fnb &&
-                    z > 0.5f * fnb && z < zm - 0.5f * fnb)
-                    continue;
-                Blob b;
-                b.x = x;
-                b.y = y;
-                b.z = z;
-                b.r = rbc->ratio * (0.2f + 0.8f * U(rng));
-                const float A = rbc->varVp * (0.5f + 0.5f * U(rng));
-                b.amp = ((rng() % 3) == 0 ? -1.0f : 1.0f) * A;
-                blobs.push_back(b);
+            BlobKey key;
+            key.seed = seed;
+            key.xm = (c->nxx - 1) * dh;
+            key.ym = (c->nyy - 1) * dh;
+            key.zm = (c->nzz - 1) * dh;
+            key.ratio = rbc->ratio;
+            key.varVp = rbc->varVp;
+            key.fnb = c->g.nb * dh;
+            // the previous call started this seed's blob set on a host thread
+            // when shots come with consecutive seeds; otherwise build it now
+            if (c->blobs_next.valid() && c->blobs_next_key == key) {
+                c->blobs_now = c->blobs_next.get();
+            } else {
+                if (c->blobs_next.valid()) c->blobs_next.wait();
+                c->blobs_now = make_blobs(key);
             }
-            if (!blobs.empty()) {
-                const float bin = 5.0f * rbc->ratio;
-                const int nbz = (int)(zm / bin) + 1, nbx = (int)(xm / bin) + 1, nby = (int)(ym / bin) + 1;
-                std::vector<std::vector<int>> bins((size_t)nbz * nbx * nby);
-                for (size_t q = 0; q < blobs.size(); ++q) {
-                    const Blob &b = blobs[q];
-                    const float e = 5.0f * b.r;
-                    auto lo = [&](float v, int nbn) { return std::max(0, std::min(nbn - 1, (int)std::floor((v - e) / bin))); };
-                    auto hi = [&](float v, int nbn) { return std::max(0, std::min(nbn - 1, (int)std::floor((v + e) / bin))); };
-                    for (int by = lo(b.y, nby); by <= hi(b.y, nby); ++by)
-                        for (int bx = lo(b.x, nbx); bx <= hi(b.x, nbx); ++bx)
-                            for (int bz = lo(b.z, nbz); bz <= hi(b.z, nbz); ++bz)
-                                bins[bz + (size_t)nbz * (bx + (size_t)nbx * by)].push_back((int)q);
-                }
-                std::vector<int> first(1, 0), list;
-                for (auto &v : bins) {
-                    list.insert(list.end(), v.begin(), v.end());
-                    first.push_back((int)list.size());
-                }
-                DevBuf<Blob> db;
-                DevBuf<int> dfirst, dlist;
-                db.ensure(blobs.size());
-                dfirst.ensure(first.size());
-                dlist.ensure(std::max<size_t>(list.size(), 1));
-                cudaError_t e = cudaMemcpyAsync(db.p, blobs.data(), blobs.size() * sizeof(Blob), cudaMemcpyHostToDevice, c->stream);
-                if (e == cudaSuccess) e = cudaMemcpyAsync(dfirst.p, first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream);
-                if (e == cudaSuccess && !list.empty()) e = cudaMemcpyAsync(dlist.p, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream);
-                if (e == cudaSuccess) {
-                    rbc_blobs_kernel<<<grid_blocks(c->vol), 256, 0, c->stream>>>(
-                        c->vp.p, c->nzz, c->nxx, c->nyy, c->ldz, c->g.nb, dh, db.p, dfirst.p, dlist.p, nbz, nbx, nby,
-                        bin, vlo, vhi);
-                    e = cudaGetLastError();
-                }
-                if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-                db.release();
-                dfirst.release();
-                dlist.release();
-                CK(e);
+            BlobKey next = key;
+            next.seed = seed + 1;
+            c->blobs_next_key = next;
+            c->blobs_next = std::async(std::launch::async, make_blobs, next);
+            const BlobSet &bs = c->blobs_now;
+            if (!bs.blobs.empty()) {
+                c->blob_dev.ensure(bs.blobs.size());
+                c->bin_first.ensure(bs.first.size());
+                c->bin_list.ensure(std::max<size_t>(bs.list.size(), 1));
+                CK(cudaMemcpyAsync(c->blob_dev.p, bs.blobs.data(), bs.blobs.size() * sizeof(Blob),
+                                   cudaMemcpyHostToDevice, c->stream));
+                CK(cudaMemcpyAsync(c->bin_first.p, bs.first.data(), bs.first.size() * sizeof(int),
+                                   cudaMemcpyHostToDevice, c->stream));
+                if (!bs.list.empty())
+                    CK(cudaMemcpyAsync(c->bin_list.p, bs.list.data(), bs.list.size() * sizeof(int),
+                                       cudaMemcpyHostToDevice, c->stream));
+                rbc_blobs_kernel<<<grid_blocks(c->vol), 256, 0, c->stream>>>(
+                    c->vp.p, c->nzz, c->nxx, c->nyy, c->ldz, c->g.nb, dh, c->blob_dev.p, c->bin_first.p,
+                    c->bin_list.p, bs.nbz, bs.nbx, bs.nby, bs.bin, vlo, vhi);
+                CK(cudaGetLastError());
                 c->launches += 1;
             }
         }
+        // check_cfl synchronises the stream, so the host vectors behind the
+        // uploads above stay valid until the copies are done
         check_cfl(c);
     });
 }
