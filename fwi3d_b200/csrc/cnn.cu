@@ -5,16 +5,22 @@
 // update.  Forward and backward run on BF16 tensor cores with FP32
 // accumulation; master weights, Adam moments and the loss are FP32 / FP64.
 //
-// Layout: activations are [V][16] BF16 (voxel v = i + nz*(j + nx*k), z fastest
-// like the model volumes, 16 channels per voxel, unused channels zero), so the
-// 16 channels of a voxel are one 32-byte row: the K dimension of each
-// implicit-GEMM tap.  Weights are [27 taps][16 co][16 ci]; tap t = (dz+1) +
-// 3 (dx+1) + 9 (dy+1).
+// Layout: activations are BF16 rows of 16 channels (32 bytes, the K of one
+// implicit-GEMM tap) over the volume padded by one zero voxel on every side:
+// row r = zp + NZ2 (xp + NX2 yp) with NZ2 = nz + 2, NX2 = nx + 2, z fastest
+// like the model volumes.  The zero halo is the convolution's "same" padding,
+// so the input rows of tap (dz, dx, dy) for output rows r0..r0+127 are the
+// contiguous rows r0 + dz + NZ2 dx + NZ2 NX2 dy + (0..127).  Weights are
+// [27 taps][16 out][16 in]; tap t = (dz+1) + 3 (dx+1) + 9 (dy+1).
 //
-// Implicit GEMM per tap: out[v][co] += in[v + off_t][ci] * W[t][co][ci].  A warp
-// owns 16 consecutive z voxels of one (x, y) column and all 16 output
-// channels: per tap two m16n8k16 BF16 MMAs (M = voxels, N = 8 channels,
-// K = 16 channels) accumulate in FP32 registers over the 27 taps.
+// Forward and data-gradient convolutions are tcgen05 kernels (conv_tc_kernel):
+// per tile of 128 output rows, TMA brings one 130-row block per (dx, dy) into
+// a shared-memory ring, and the three z taps of that block are three
+// MMAs whose weights hold the three z taps side by side (N = 48).  The weight
+// gradient (wgrad_tc_kernel) is a tcgen05 reduction over rows into tensor
+// memory.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -26,33 +32,62 @@
 #include <vector>
 
 #include "../../include/fwi3d.h"
+#include "device.cuh"
 
 namespace {
+
+using fwi::mbar_arrive;
+using fwi::mbar_expect_tx;
+using fwi::mbar_init;
+using fwi::mbar_wait;
+using fwi::smem_addr;
 
 constexpr int CH = 16;     // channels per voxel row
 constexpr int NL = 4;      // layers
 constexpr int TAPS = 27;
 constexpr int WSZ = TAPS * CH * CH;  // weights per layer
 constexpr int CIN[NL] = {3, 16, 16, 16};
+constexpr int kMaxPartials = 1024;  // per-CTA weight-gradient partials held
 constexpr int COUT[NL] = {16, 16, 16, 1};
-constexpr int WARPS = 8;   // warps per CTA in the conv kernels
+
+// Division by a run-time invariant d (1 <= d < 2^31) of dividends n < 2^31,
+// by multiplication (Granlund & Montgomery, "Division by invariant integers
+// using multiplication", PLDI 1994): with s = ceil(log2 d) and
+// m = floor(2^32 (2^s - d) / d) + 1, n / d = (umulhi(n, m) + n) >> s.
+struct FastDiv {
+    uint32_t d = 1, m = 1, s = 0;
+};
+
+FastDiv make_fastdiv(uint32_t d)
+{
+    FastDiv f;
+    f.d = d;
+    while ((1ull << f.s) < d) ++f.s;
+    f.m = (uint32_t)(((1ull << 32) * ((1ull << f.s) - d)) / d + 1);
+    return f;
+}
+
+__device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv &f) { return (__umulhi(n, f.m) + n) >> f.s; }
 
 struct Geo {
     int nz, nx, ny;
-    long long V;
+    long long V;      // interior voxels
+    int NZ2, NX2;     // padded z and x extents
+    long long R;      // padded rows (nz+2)(nx+2)(ny+2), below 2^31
+    FastDiv fz, fx;   // division by NZ2 and NX2
 };
 
-__device__ __forceinline__ uint32_t ld_b32(const __nv_bfloat16 *p) { return *reinterpret_cast<const uint32_t *>(p); }
-
-__device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
-                                         uint32_t b0, uint32_t b1)
+// Interior voxel of padded row r, or -1 on the halo.
+__device__ __forceinline__ long long interior_of(const Geo &g, long long r)
 {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+    const uint32_t rr = (uint32_t)r;
+    const uint32_t rest = fdiv(rr, g.fz), yp = fdiv(rest, g.fx);
+    const int zp = (int)(rr - rest * (uint32_t)g.NZ2), xp = (int)(rest - yp * (uint32_t)g.NX2);
+    if (zp < 1 || zp > g.nz || xp < 1 || xp > g.nx || yp < 1 || (int)yp > g.ny) return -1;
+    return (zp - 1) + (long long)g.nz * ((xp - 1) + (long long)g.nx * ((int)yp - 1));
 }
+
+__device__ unsigned int g_cnn_status;  // bit 0: a bounded wait gave up
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 {
@@ -61,223 +96,551 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 }
 
 // ---------------------------------------------------------------------------
-// Convolution over all 27 taps.  SIGN = +1: forward (out[v] = sum in[v+off] W);
-// SIGN = -1: data gradient (dx[v] = sum dy[v-off] W^T, W given transposed).
-// MODE 0: BF16 [V][16] output with bias and ReLU; 1: BF16 [V][16] output times
-// the ReLU mask of `mask` (data gradient through the previous activation);
-// 2: FP32 channel-0 output with bias (last layer, no activation).
+// tcgen05 convolution over all 27 taps.
+// SIGN = +1: forward, out[r] = sum_t in[r + off_t] W_t;
+// SIGN = -1: data gradient, dx[r] = sum_t dy[r - off_t] W_t^T (w = W transposed).
+// MODE 0: BF16 rows with bias and ReLU; 1: BF16 rows times the ReLU mask of
+// `mask` (data gradient through the previous activation); 2: FP32 channel 0
+// with bias into the unpadded volume (last layer, no activation).  Halo rows
+// of BF16 outputs are written as zeros, so every output is again a padded
+// input.
+//
+// A tile is 126 output rows r0..r0+125.  For each (dx, dy) one TMA load brings
+// the 128 input rows r0 + SIGN (dx NZ2 + dy NZ2 NX2) - 1 + i (i = 0..127), and
+// one MMA (M = 128 rows, N = 48, K = 16 channels) multiplies them by the
+// weights of the three z taps side by side: column group k holds z tap
+// dz = SIGN (k - 1), and group k of block row m + k feeds output row m:
+//     out[r0 + m] = D[m][group 0] + D[m+1][group 1] + D[m+2][group 2].
+// Nine MMAs per tile; the epilogue adds the three groups across rows (warp
+// shuffles, plus a small shared exchange for the two rows that cross a warp
+// boundary).
+//
+// Warp 0 issues the TMA loads, warp 1 allocates tensor memory and issues the
+// MMAs, warps 2..5 drain the accumulators (warp w reads TMEM lanes 32 (w%4)..).
+// Two accumulators alternate, so the epilogue of one tile overlaps the MMAs of
+// the next, and four CTAs share an SM's tensor pipe.  Every wait is bounded; a
+// wait that gives up sets g_cnn_status, and the kernel drains its copies and
+// MMAs, frees its tensor memory and returns.
 // ---------------------------------------------------------------------------
+namespace tc {
+constexpr int BM = 128;                       // input rows per block (MMA M)
+constexpr int TM = BM - 2;                    // output rows per tile
+constexpr int PLANE = BM * 16;                // bytes of one 8-channel half of a block
+constexpr int SLOT = 2 * PLANE;
+constexpr int NS = 9;                         // ring slots (a tile takes 9)
+constexpr int NG = 3 * CH;                    // MMA N: (z tap, channel)
+constexpr int BJ = NG * CH * 2;               // bytes of the B operand of one (dx, dy)
+constexpr int WBYTES = 9 * BJ;
+constexpr int XBYTES = 2 * 4 * 2 * 32 * 4;    // [tile parity][warp][row][32 floats]
+constexpr int THREADS = 192;
+constexpr int CTAS_PER_SM = 4;                // registers: 4 x 192 threads x 80
+constexpr uint32_t ACC_STRIDE = 64;           // TMEM columns between the two accumulators
+constexpr uint32_t TMEM_COLS = 128;
+constexpr uint32_t LOAD_BYTES = SLOT;
+constexpr int BAR_BYTES = (2 * NS + 5) * 8;
+constexpr int SMEM = NS * SLOT + WBYTES + XBYTES + BAR_BYTES + 16 + CH * 4;
+constexpr uint32_t IDESC = fwi::umma_idesc_bf16(BM, NG);
+static_assert(NS < 32, "slot bitmasks");
+static_assert(BM <= 256, "TMA box dimension limit");
+static_assert(NG <= (int)ACC_STRIDE, "accumulator columns");
+}  // namespace tc
+
+struct ConvArgs {
+    Geo g;
+    int ntiles;
+    const __nv_bfloat16 *w;     // [27][16 n][16 k]: B operand rows n, K = k
+    const float *bias;          // [16] (MODE 0, 2)
+    const __nv_bfloat16 *mask;  // padded rows (MODE 1)
+    __nv_bfloat16 *out;         // padded rows (MODE 0, 1)
+    float *out32;               // unpadded volume (MODE 2)
+};
+
+__device__ __forceinline__ void cnn_fail(volatile int *abort_flag)
+{
+    *abort_flag = 1;
+    atomicOr(&g_cnn_status, 1u);
+}
+
 template <int SIGN, int MODE>
-__global__ void __launch_bounds__(WARPS * 32)
-    conv_kernel(Geo g, const __nv_bfloat16 *__restrict__ in, const __nv_bfloat16 *__restrict__ w,
-                const float *__restrict__ bias, const __nv_bfloat16 *__restrict__ mask,
-                __nv_bfloat16 *__restrict__ out, float *__restrict__ out32)
+__global__ void __launch_bounds__(tc::THREADS, tc::CTAS_PER_SM)
+    conv_tc_kernel(const __grid_constant__ CUtensorMap map, const ConvArgs a)
 {
-    __shared__ __align__(16) __nv_bfloat16 ws[WSZ];
-    for (int i = threadIdx.x; i < WSZ / 8; i += blockDim.x)
-        reinterpret_cast<uint4 *>(ws)[i] = reinterpret_cast<const uint4 *>(w)[i];
+    using namespace tc;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char *ring = smem;
+    unsigned char *wsm = smem + NS * SLOT;
+    float *xch = reinterpret_cast<float *>(wsm + WBYTES);
+    uint64_t *full = reinterpret_cast<uint64_t *>(wsm + WBYTES + XBYTES);
+    uint64_t *empty = full + NS;
+    uint64_t *accf = empty + NS;  // [2] accumulator ready
+    uint64_t *acce = accf + 2;    // [2] accumulator drained
+    uint64_t *done = acce + 2;    // every MMA of this CTA completed
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+    float *bsm = reinterpret_cast<float *>(wsm + WBYTES + XBYTES + BAR_BYTES + 16);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if ((smem_addr(smem) & 127u) != 0u) {  // TMA destinations need 128-byte alignment
+        if (threadIdx.x == 0) atomicOr(&g_cnn_status, 2u);
+        return;
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < NS; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&accf[b], 1);
+            mbar_init(&acce[b], 4);
+        }
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        fwi::fence_mbar_init();
+    }
+    // B operand of (dx, dy) = j: rows n = 16 k + c_out, k = z-tap group, from
+    // w[t][c_out][:] with t = (dz+1) + 3 (dx+1) + 9 (dy+1), dz = SIGN (k-1);
+    // stored [j][K half][n][8]: K-major core matrices of 8 rows x 16 bytes,
+    // the two K halves NG*16 bytes apart
+    for (int i = threadIdx.x; i < 9 * NG * 2; i += blockDim.x) {
+        const int j = i / (NG * 2), n = (i >> 1) % NG, c = i & 1;
+        const int k = n / CH, co = n % CH;
+        const int dz = SIGN * (k - 1), dx = j % 3 - 1, dy = j / 3 - 1;
+        const int t = (dz + 1) + 3 * (dx + 1) + 9 * (dy + 1);
+        const uint4 v = *reinterpret_cast<const uint4 *>(a.w + (t * CH + co) * CH + c * 8);
+        *reinterpret_cast<uint4 *>(wsm + j * BJ + c * (NG * 16) + n * 16) = v;
+    }
+    if (threadIdx.x < CH) bsm[threadIdx.x] = a.bias ? a.bias[threadIdx.x] : 0.0f;
+    fwi::fence_proxy_async();  // the tensor core reads what the threads wrote
+    if (warp == 1) fwi::tmem_alloc(tmem_slot, TMEM_COLS);
+    fwi::tc_fence_before();
     __syncthreads();
+    fwi::tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const long long plane_xy = (long long)a.g.NZ2 * a.g.NX2;
 
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int grp = lane >> 2, q = lane & 3;
-    const int nzt = (g.nz + 15) / 16;
-    const long long ntiles = (long long)nzt * g.nx * g.ny;
-    for (long long tile = (long long)blockIdx.x * WARPS + warp; tile < ntiles; tile += (long long)gridDim.x * WARPS) {
-        const int zt = (int)(tile % nzt);
-        const long long col = tile / nzt;
-        const int j = (int)(col % g.nx), k = (int)(col / g.nx);
-        const int z0 = zt * 16;
-        float acc0[4] = {0, 0, 0, 0}, acc1[4] = {0, 0, 0, 0};
-        for (int dy = -1; dy <= 1; ++dy) {
-            const int kk = k + SIGN * dy;
-            if (kk < 0 || kk >= g.ny) continue;
-            for (int dx = -1; dx <= 1; ++dx) {
-                const int jj = j + SIGN * dx;
-                if (jj < 0 || jj >= g.nx) continue;
-                const long long cbase = ((long long)kk * g.nx + jj) * g.nz;
-#pragma unroll
-                for (int dz = -1; dz <= 1; ++dz) {
-                    const int t = (dz + 1) + 3 * (dx + 1) + 9 * (dy + 1);
-                    const int za = z0 + grp + SIGN * dz, zb = za + 8;
-                    const bool va = za >= 0 && za < g.nz, vb = zb >= 0 && zb < g.nz;
-                    const __nv_bfloat16 *ra = in + (cbase + za) * CH + 2 * q;
-                    const __nv_bfloat16 *rb = in + (cbase + zb) * CH + 2 * q;
-                    const uint32_t a0 = va ? ld_b32(ra) : 0u, a2 = va ? ld_b32(ra + 8) : 0u;
-                    const uint32_t a1 = vb ? ld_b32(rb) : 0u, a3 = vb ? ld_b32(rb + 8) : 0u;
-                    const __nv_bfloat16 *wt = ws + t * CH * CH + grp * CH + 2 * q;
-                    mma_bf16(acc0, a0, a1, a2, a3, ld_b32(wt), ld_b32(wt + 8));
-                    mma_bf16(acc1, a0, a1, a2, a3, ld_b32(wt + 8 * CH), ld_b32(wt + 8 * CH + 8));
-                }
-            }
-        }
-        const long long base = ((long long)k * g.nx + j) * g.nz;
-        const int za = z0 + grp, zb = za + 8;
-        if constexpr (MODE == 2) {
-            // last layer: only output channel 0 is real (thread q == 0 of n-tile 0)
-            if (q == 0) {
-                if (za < g.nz) out32[base + za] = acc0[0] + bias[0];
-                if (zb < g.nz) out32[base + zb] = acc0[2] + bias[0];
-            }
-        } else {
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int z = h ? zb : za;
-            if (z >= g.nz) continue;
-            const long long v = base + z;
-#pragma unroll
-            for (int nt = 0; nt < 2; ++nt) {
-                const float *acc = nt ? acc1 : acc0;
-                const int co = nt * 8 + 2 * q;
-                float x0 = acc[2 * h], x1 = acc[2 * h + 1];
-                if (MODE == 0) {
-                    x0 = fmaxf(x0 + bias[co], 0.0f);
-                    x1 = fmaxf(x1 + bias[co + 1], 0.0f);
-                } else {
-                    const __nv_bfloat162 m = *reinterpret_cast<const __nv_bfloat162 *>(mask + v * CH + co);
-                    if (!(__bfloat162float(m.x) > 0.0f)) x0 = 0.0f;
-                    if (!(__bfloat162float(m.y) > 0.0f)) x1 = 0.0f;
-                }
-                *reinterpret_cast<uint32_t *>(out + v * CH + co) = pack_bf16(x0, x1);
-            }
-        }
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Weight gradient: dW[t][co][ci] = sum_v dy[v][co] x[v + off_t][ci], as
-// M = co (16) x N = ci (16) x K = voxels MMAs.  Warp w of a CTA owns taps
-// 3w..3w+2 over the CTA's columns, so every partial is written by one warp
-// (no atomics); partials [cta][27][16][16] are summed in a fixed order by
-// reduce_partials_kernel.  Bias gradient partials ride along in warp 0.
-// ---------------------------------------------------------------------------
-constexpr int WG_WARPS = 9;
-
-__global__ void __launch_bounds__(WG_WARPS * 32)
-    conv_wgrad_kernel(Geo g, const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__restrict__ dy,
-                      int cols_per_cta, float *__restrict__ partial, float *__restrict__ bpartial)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int grp = lane >> 2, q = lane & 3;
-    const long long ncols = (long long)g.nx * g.ny;
-    const long long c0 = (long long)blockIdx.x * cols_per_cta;
-    const long long c1 = c0 + cols_per_cta < ncols ? c0 + cols_per_cta : ncols;
-    float acc[3][2][4];
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int b = 0; b < 2; ++b)
-#pragma unroll
-            for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0f;
-    float bacc = 0.0f;
-    const int tdy = warp / 3 - 1, tdx = warp % 3 - 1;  // taps (dz, tdx, tdy), dz = -1..1
-    for (long long col = c0; col < c1; ++col) {
-        const int j = (int)(col % g.nx), k = (int)(col / g.nx);
-        const long long base = ((long long)k * g.nx + j) * g.nz;
-        const int jj = j + tdx, kk = k + tdy;
-        const bool cin = jj >= 0 && jj < g.nx && kk >= 0 && kk < g.ny;
-        const long long xbase = ((long long)kk * g.nx + jj) * g.nz;
-        for (int z0 = 0; z0 < g.nz; z0 += 16) {
-            // A (m = co, k = voxel): rows grp, grp+8; voxels 2q, 2q+1, 2q+8, 2q+9
-            uint32_t a[4];
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                const int co = grp + (r & 1) * 8;
-                const int zv = z0 + 2 * q + (r >> 1) * 8;
-                const float lo = zv < g.nz ? __bfloat162float(dy[(base + zv) * CH + co]) : 0.0f;
-                const float hi = zv + 1 < g.nz ? __bfloat162float(dy[(base + zv + 1) * CH + co]) : 0.0f;
-                a[r] = pack_bf16(lo, hi);
-            }
-            if (!cin) continue;
-#pragma unroll
-            for (int dz = -1; dz <= 1; ++dz) {
-#pragma unroll
-                for (int nt = 0; nt < 2; ++nt) {
-                    // B (k = voxel, n = ci): voxels 2q, 2q+1 (+8), channel nt*8 + grp
-                    const int ci = nt * 8 + grp;
-                    uint32_t b[2];
-#pragma unroll
-                    for (int r = 0; r < 2; ++r) {
-                        // K index z (voxel of dy) reads x at z + dz of the shifted column
-                        float vals[2];
-#pragma unroll
-                        for (int h = 0; h < 2; ++h) {
-                            const int z = z0 + 2 * q + r * 8 + h, zx = z + dz;
-                            vals[h] = (z < g.nz && zx >= 0 && zx < g.nz)
-                                          ? __bfloat162float(x[(xbase + zx) * CH + ci]) : 0.0f;
-                        }
-                        b[r] = pack_bf16(vals[0], vals[1]);
-                    }
-                    mma_bf16(acc[dz + 1][nt], a[0], a[1], a[2], a[3], b[0], b[1]);
-                }
-            }
-        }
-        if (warp == 0) {
-            // bias gradient: lane l sums channel l & 15 over half of the column
-            const int co = lane & 15;
-            for (int z = lane >> 4; z < g.nz; z += 2) bacc += __bfloat162float(dy[(base + z) * CH + co]);
-        }
-    }
-    float *P = partial + (long long)blockIdx.x * WSZ;
-#pragma unroll
-    for (int dz = -1; dz <= 1; ++dz) {
-        const int t = (dz + 1) + 3 * (tdx + 1) + 9 * (tdy + 1);
-#pragma unroll
-        for (int nt = 0; nt < 2; ++nt) {
-            const float *c = acc[dz + 1][nt];
-            const int ci = nt * 8 + 2 * q;
-            P[t * CH * CH + grp * CH + ci] = c[0];
-            P[t * CH * CH + grp * CH + ci + 1] = c[1];
-            P[t * CH * CH + (grp + 8) * CH + ci] = c[2];
-            P[t * CH * CH + (grp + 8) * CH + ci + 1] = c[3];
-        }
-    }
     if (warp == 0) {
-        bacc += __shfl_down_sync(0xffffffffu, bacc, 16);
-        if (lane < 16) bpartial[(long long)blockIdx.x * CH + lane] = bacc;
+        if (lane == 0) {
+            // producer: one 128-row block per (dx, dy); rows outside the
+            // tensor read as zeros
+            fwi::prefetch_tmap(&map);
+            uint32_t used = 0, phases = 0;
+            int slot = 0;
+            uint32_t ph = 0;
+            for (long long tile = blockIdx.x; tile < a.ntiles && !*abort_flag; tile += gridDim.x) {
+                const long long r0 = tile * TM;
+                for (int j = 0; j < 9; ++j) {
+                    const int dx = j % 3 - 1, dy = j / 3 - 1;
+                    if (!mbar_wait(&empty[slot], ph ^ 1u)) {
+                        cnn_fail(abort_flag);
+                        break;
+                    }
+                    mbar_expect_tx(&full[slot], LOAD_BYTES);
+                    const long long start = r0 + SIGN * (dx * (long long)a.g.NZ2 + dy * plane_xy) - 1;
+                    fwi::tma_load_3d(ring + slot * SLOT, &map, &full[slot], 0, (int)start, 0);
+                    used |= 1u << slot;
+                    phases = (phases & ~(1u << slot)) | (ph << slot);
+                    if (++slot == NS) {
+                        slot = 0;
+                        ph ^= 1u;
+                    }
+                }
+            }
+            // no copy may land after the CTA has gone
+            for (int s = 0; s < NS; ++s)
+                if ((used >> s) & 1u)
+                    if (!mbar_wait(&full[s], (phases >> s) & 1u)) atomicOr(&g_cnn_status, 1u);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // MMA issuer
+            const uint32_t ring_a = smem_addr(ring), w_a = smem_addr(wsm);
+            int slot = 0;
+            uint32_t ph = 0;
+            int it = 0;
+            for (long long tile = blockIdx.x; tile < a.ntiles && !*abort_flag; tile += gridDim.x, ++it) {
+                const int buf = it & 1;
+                if (!mbar_wait(&acce[buf], (((uint32_t)it >> 1) & 1u) ^ 1u)) {
+                    cnn_fail(abort_flag);
+                    break;
+                }
+                fwi::tc_fence_after();
+                const uint32_t d = tmem + (uint32_t)buf * ACC_STRIDE;
+                bool ok = true;
+                for (int j = 0; j < 9; ++j) {
+                    if (!mbar_wait(&full[slot], ph)) {
+                        cnn_fail(abort_flag);
+                        ok = false;
+                        break;
+                    }
+                    fwi::tc_fence_after();
+                    const uint64_t ad = fwi::umma_desc(ring_a + slot * SLOT, PLANE, 128);
+                    const uint64_t bd = fwi::umma_desc(w_a + j * BJ, NG * 16, 128);
+                    fwi::umma_bf16(d, ad, bd, IDESC, j > 0 ? 1u : 0u);
+                    fwi::umma_commit(&empty[slot]);
+                    if (++slot == NS) {
+                        slot = 0;
+                        ph ^= 1u;
+                    }
+                }
+                if (!ok) break;
+                fwi::umma_commit(&accf[buf]);
+            }
+            fwi::umma_commit(done);
+            if (!mbar_wait(done, 0)) atomicOr(&g_cnn_status, 1u);
+        }
+    } else {
+        // epilogue: accumulator row 32 q + lane, q = warp % 4.  Every epilogue
+        // thread reaches the named barrier once per tile; its AND decides
+        // together whether all four warps go on (tcgen05.ld is
+        // warp-collective, bar.red is block-partial: both need uniform exits)
+        const int q = warp & 3;
+        int it = 0;
+        for (long long tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++it) {
+            const int buf = it & 1;
+            bool ok = *abort_flag == 0 && mbar_wait(&accf[buf], ((uint32_t)it >> 1) & 1u);
+            ok = __all_sync(0xffffffffu, ok);
+            uint32_t v0[16], v1[16], v2[16];
+            float *xb = xch + (it & 1) * (4 * 2 * 32);
+            if (ok) {
+                fwi::tc_fence_after();
+                const uint32_t t0 = tmem + (uint32_t)buf * ACC_STRIDE + ((uint32_t)(32 * q) << 16);
+                fwi::tmem_ld16(t0, v0);
+                fwi::tmem_ld16(t0 + CH, v1);
+                fwi::tmem_ld16(t0 + 2 * CH, v2);
+                fwi::tmem_wait_ld();
+                fwi::tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&acce[buf]);
+                // rows 32q and 32q+1 also feed the two last rows of warp q-1
+                if (q >= 1 && lane < 2) {
+#pragma unroll
+                    for (int c = 0; c < CH; ++c) {
+                        xb[(q * 2 + lane) * 32 + c] = __uint_as_float(v1[c]);
+                        xb[(q * 2 + lane) * 32 + CH + c] = __uint_as_float(v2[c]);
+                    }
+                }
+            }
+            if (!fwi::bar_and(1, 128, ok)) {
+                if (lane == 0 && ok) cnn_fail(abort_flag);
+                break;
+            }
+            // output row m = D[m][0:16] + D[m+1][16:32] + D[m+2][32:48]
+            const int m = 32 * q + lane;
+            float o[CH];
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                float b1 = __shfl_down_sync(0xffffffffu, __uint_as_float(v1[c]), 1);
+                float b2 = __shfl_down_sync(0xffffffffu, __uint_as_float(v2[c]), 2);
+                if (q < 3) {
+                    if (lane == 31) b1 = xb[((q + 1) * 2) * 32 + c];
+                    if (lane >= 30) b2 = xb[((q + 1) * 2 + lane - 30) * 32 + CH + c];
+                }
+                o[c] = (__uint_as_float(v0[c]) + b1) + b2;
+            }
+            const long long r = tile * TM + m;
+            if (m >= TM || r >= a.g.R) continue;
+            const long long vox = interior_of(a.g, r);
+            if constexpr (MODE == 2) {
+                if (vox >= 0) a.out32[vox] = o[0] + bsm[0];
+            } else {
+                uint32_t pk[8];
+                if (vox < 0) {
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) pk[c] = 0u;
+                } else {
+                    uint32_t mk[8];
+                    if constexpr (MODE == 1) {
+                        const uint4 m0 = reinterpret_cast<const uint4 *>(a.mask + r * CH)[0];
+                        const uint4 m1 = reinterpret_cast<const uint4 *>(a.mask + r * CH)[1];
+                        mk[0] = m0.x; mk[1] = m0.y; mk[2] = m0.z; mk[3] = m0.w;
+                        mk[4] = m1.x; mk[5] = m1.y; mk[6] = m1.z; mk[7] = m1.w;
+                    }
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) {
+                        float x0 = o[2 * c], x1 = o[2 * c + 1];
+                        if constexpr (MODE == 0) {
+                            x0 = fmaxf(x0 + bsm[2 * c], 0.0f);
+                            x1 = fmaxf(x1 + bsm[2 * c + 1], 0.0f);
+                        } else {
+                            __nv_bfloat162 mm;
+                            *reinterpret_cast<uint32_t *>(&mm) = mk[c];
+                            if (!(__bfloat162float(mm.x) > 0.0f)) x0 = 0.0f;
+                            if (!(__bfloat162float(mm.y) > 0.0f)) x1 = 0.0f;
+                        }
+                        pk[c] = pack_bf16(x0, x1);
+                    }
+                }
+                uint4 *dst = reinterpret_cast<uint4 *>(a.out + r * CH);
+                dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+            }
+        }
+    }
+    fwi::tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        fwi::tc_fence_after();
+        fwi::tmem_dealloc(tmem, TMEM_COLS);
     }
 }
 
-// Fixed-order sum of per-CTA partials: out[i] = sum_b part[b][i].
-__global__ void reduce_partials_kernel(const float *__restrict__ part, int nb, int n, float *__restrict__ out)
+// ---------------------------------------------------------------------------
+// tcgen05 weight gradient.
+//   dW[t][co][ci] = sum_v dy[v][co] x[v + off_t][ci]
+//                 = sum_u dy[u - dz][co] x[u + NZ2 dx + NZ2 NX2 dy][ci]   (u = v + dz)
+// over every padded row (halo rows of dy are zero).  Each CTA owns a range of
+// 128-row blocks of u.  Per block, TMA brings the x rows of the nine (dx, dy)
+// offsets and the dy rows u-1 .. u+130; both operands are MN-major (channels
+// contiguous), no swizzle.
+//   - Group 1: the x blocks of offsets 0..7 stacked along M (M = 8 x 16 ci).
+//   - Group 2: the x block of offset 8, then a block of ones in channel 0
+//     (M rows 16..31), then six blocks of group 1 whose rows are not used.
+//     Row 16 with dz = 0 is sum_u dy[u][co]: the bias gradient.
+// The z tap is the dy descriptor's start row (dz = -1, 0, 1 -> rows +2, +1,
+// +0), so each 16-row K step is six MMAs (M = 128, N = 16, K = 16) into six
+// accumulators that live in tensor memory for the whole row range.  The
+// epilogue writes per-CTA partials [cta][27][16 co][16 ci] and [cta][16],
+// summed in a fixed order by reduce_partials_kernel.
+// ---------------------------------------------------------------------------
+namespace wg {
+constexpr int BK = 128;                        // rows of u per block (K)
+constexpr int APLANE = BK * 16;                // one channel half of an x block
+constexpr int ABLK = 2 * APLANE;
+constexpr int BROWS = BK + 4;                  // dy rows u-1 .. u+130
+constexpr int BPLANE = BROWS * 16;
+constexpr int BBLK = 2 * BPLANE;
+constexpr int OFF_B8 = 0, OFF_ONES = ABLK, OFF_G1 = 2 * ABLK, OFF_DY = 10 * ABLK;
+constexpr int STAGE = 10 * ABLK + BBLK;
+constexpr int NSTAGE = 2;
+constexpr int THREADS = 192;
+constexpr int CTAS_PER_SM = 2;
+constexpr int NACC = 6;                        // 2 groups x 3 z taps
+constexpr uint32_t TMEM_COLS = 128;
+constexpr uint32_t LOAD_BYTES = 9 * ABLK + BBLK;
+constexpr int BAR_BYTES = (2 * NSTAGE + 1) * 8;
+constexpr int SMEM = NSTAGE * STAGE + BAR_BYTES + 16;
+constexpr uint32_t IDESC = fwi::umma_idesc_bf16(128, CH, true, true);
+static_assert(STAGE % 128 == 0, "TMA destinations need 128-byte alignment");
+static_assert(NACC * CH <= (int)TMEM_COLS, "accumulator columns");
+}  // namespace wg
+
+struct WgradArgs {
+    Geo g;
+    int nkb;           // 128-row blocks of u
+    int kb_per_cta;
+    float *partial;    // [gridDim.x][27][16][16]
+    float *bpartial;   // [gridDim.x][16]
+};
+
+__global__ void __launch_bounds__(wg::THREADS, wg::CTAS_PER_SM)
+    wgrad_tc_kernel(const __grid_constant__ CUtensorMap mx, const __grid_constant__ CUtensorMap mdy,
+                    const WgradArgs a)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        float s = 0.0f;
-        for (int b = 0; b < nb; ++b) s += part[(long long)b * n + i];
-        out[i] = s;
+    using namespace wg;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + NSTAGE * STAGE);
+    uint64_t *empty = full + NSTAGE;
+    uint64_t *done = empty + NSTAGE;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if ((smem_addr(smem) & 127u) != 0u) {
+        if (threadIdx.x == 0) atomicOr(&g_cnn_status, 2u);
+        return;
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < NSTAGE; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        fwi::fence_mbar_init();
+    }
+    // the ones block of every stage: channel 0 = 1 in every row (MN-major:
+    // plane 0 holds channels 0..7 of rows 0..127, 16 bytes per row)
+    for (int i = threadIdx.x; i < NSTAGE * ABLK / 16; i += blockDim.x) {
+        const int st = i / (ABLK / 16), k = i % (ABLK / 16);
+        const uint4 one = make_uint4(k < BK ? 0x3F80u : 0u, 0u, 0u, 0u);  // BF16 1.0 in the low half
+        *reinterpret_cast<uint4 *>(smem + st * STAGE + OFF_ONES + k * 16) = one;
+    }
+    fwi::fence_proxy_async();
+    if (warp == 1) fwi::tmem_alloc(tmem_slot, TMEM_COLS);
+    fwi::tc_fence_before();
+    __syncthreads();
+    fwi::tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const long long kb0 = (long long)blockIdx.x * a.kb_per_cta;
+    const long long kb1 = kb0 + a.kb_per_cta < a.nkb ? kb0 + a.kb_per_cta : a.nkb;
+    const long long plane_xy = (long long)a.g.NZ2 * a.g.NX2;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            fwi::prefetch_tmap(&mx);
+            fwi::prefetch_tmap(&mdy);
+            uint32_t used = 0, phases = 0;
+            int st = 0;
+            uint32_t ph = 0;
+            for (long long kb = kb0; kb < kb1 && !*abort_flag; ++kb) {
+                if (!mbar_wait(&empty[st], ph ^ 1u)) {
+                    cnn_fail(abort_flag);
+                    break;
+                }
+                unsigned char *base = smem + st * STAGE;
+                mbar_expect_tx(&full[st], LOAD_BYTES);
+                const long long u0 = kb * BK;
+                for (int j = 0; j < 9; ++j) {
+                    const int dx = j % 3 - 1, dy = j / 3 - 1;
+                    const long long r = u0 + dx * (long long)a.g.NZ2 + dy * plane_xy;
+                    fwi::tma_load_3d(base + (j < 8 ? OFF_G1 + j * ABLK : OFF_B8), &mx, &full[st], 0, (int)r, 0);
+                }
+                fwi::tma_load_3d(base + OFF_DY, &mdy, &full[st], 0, (int)(u0 - 1), 0);
+                used |= 1u << st;
+                phases = (phases & ~(1u << st)) | (ph << st);
+                if (++st == NSTAGE) {
+                    st = 0;
+                    ph ^= 1u;
+                }
+            }
+            for (int s = 0; s < NSTAGE; ++s)
+                if ((used >> s) & 1u)
+                    if (!mbar_wait(&full[s], (phases >> s) & 1u)) atomicOr(&g_cnn_status, 1u);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t s_a = smem_addr(smem);
+            int st = 0;
+            uint32_t ph = 0;
+            bool first = true;
+            for (long long kb = kb0; kb < kb1 && !*abort_flag; ++kb) {
+                if (!mbar_wait(&full[st], ph)) {
+                    cnn_fail(abort_flag);
+                    break;
+                }
+                fwi::tc_fence_after();
+                const uint32_t base = s_a + st * STAGE;
+#pragma unroll 1
+                for (int s = 0; s < BK / 16; ++s) {
+                    const uint32_t koff = s * 256;  // 16 rows = two 8-row K groups
+#pragma unroll
+                    for (int g = 0; g < 2; ++g) {
+                        const uint64_t ad = fwi::umma_desc(base + (g ? OFF_B8 : OFF_G1) + koff, 128, APLANE);
+#pragma unroll
+                        for (int dz = -1; dz <= 1; ++dz) {
+                            const uint64_t bd = fwi::umma_desc(base + OFF_DY + (1 - dz) * 16 + koff, 128, BPLANE);
+                            fwi::umma_bf16(tmem + (uint32_t)(3 * g + dz + 1) * CH, ad, bd, IDESC,
+                                           (first && s == 0) ? 0u : 1u);
+                        }
+                    }
+                }
+                first = false;
+                fwi::umma_commit(&empty[st]);
+                if (++st == NSTAGE) {
+                    st = 0;
+                    ph ^= 1u;
+                }
+            }
+            fwi::umma_commit(done);
+        }
+    } else {
+        // epilogue: wait for the last MMA, then TMEM lanes 32 q .. 32 q + 31
+        const int q = warp & 3;
+        const bool ok = __all_sync(0xffffffffu, mbar_wait(done, 0));
+        if (ok) {
+            fwi::tc_fence_after();
+            const bool empty_range = kb0 >= kb1;
+            const int m = 32 * q + lane;  // accumulator row
+            float *P = a.partial + (long long)blockIdx.x * WSZ;
+#pragma unroll 1
+            for (int acc = 0; acc < NACC; ++acc) {
+                uint32_t v[16];
+                fwi::tmem_ld16(tmem + (uint32_t)acc * CH + ((uint32_t)(32 * q) << 16), v);
+                fwi::tmem_wait_ld();
+                const int g = acc / 3, dz = acc % 3 - 1;
+                int j = -1, ci = m % CH;
+                if (g == 0) j = m / CH;
+                else if (m < CH) j = 8;
+                if (j >= 0) {
+                    const int t = (dz + 1) + 3 * (j % 3) + 9 * (j / 3);
+#pragma unroll
+                    for (int co = 0; co < CH; ++co)
+                        P[(t * CH + co) * CH + ci] = empty_range ? 0.0f : __uint_as_float(v[co]);
+                }
+                if (g == 1 && dz == 0 && m == CH) {
+#pragma unroll
+                    for (int co = 0; co < CH; ++co)
+                        a.bpartial[(long long)blockIdx.x * CH + co] = empty_range ? 0.0f : __uint_as_float(v[co]);
+                }
+            }
+        } else if (lane == 0) {
+            cnn_fail(abort_flag);
+        }
+    }
+    fwi::tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        fwi::tc_fence_after();
+        fwi::tmem_dealloc(tmem, TMEM_COLS);
     }
 }
 
-// Pack three FP32 channel volumes into the BF16 [V][16] input rows.
-__global__ void pack_input_kernel(long long V, const float *__restrict__ c0, const float *__restrict__ c1,
+// Fixed-order sum of per-CTA partials: out[i] = sum_b part[b][i].  A block
+// is 32 entries x 8 slices of b; slice y sums b = y, y+8, ... in order, then
+// the eight slice sums are added in order.
+constexpr int RED_X = 32, RED_Y = 8;
+
+__global__ void __launch_bounds__(RED_X * RED_Y)
+    reduce_partials_kernel(const float *__restrict__ part, int nb, int n, float *__restrict__ out)
+{
+    __shared__ float red[RED_Y][RED_X];
+    const int x = threadIdx.x % RED_X, y = threadIdx.x / RED_X;
+    const int i = blockIdx.x * RED_X + x;
+    float s = 0.0f;
+    if (i < n)
+        for (int b = y; b < nb; b += RED_Y) s += part[(long long)b * n + i];
+    red[y][x] = s;
+    __syncthreads();
+    if (y == 0 && i < n) {
+        float t = red[0][x];
+        for (int k = 1; k < RED_Y; ++k) t += red[k][x];
+        out[i] = t;
+    }
+}
+
+// Pack three FP32 channel volumes into the BF16 input rows (zero halo).
+__global__ void pack_input_kernel(Geo g, const float *__restrict__ c0, const float *__restrict__ c1,
                                   const float *__restrict__ c2, __nv_bfloat16 *__restrict__ out)
 {
-    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < V; v += (long long)gridDim.x * blockDim.x) {
-        uint4 r0, r1;
-        r0.x = pack_bf16(c0[v], c1[v]);
-        r0.y = pack_bf16(c2[v], 0.0f);
-        r0.z = r0.w = 0u;
-        r1.x = r1.y = r1.z = r1.w = 0u;
-        reinterpret_cast<uint4 *>(out + v * CH)[0] = r0;
-        reinterpret_cast<uint4 *>(out + v * CH)[1] = r1;
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < g.R; r += (long long)gridDim.x * blockDim.x) {
+        const long long v = interior_of(g, r);
+        uint4 r0 = make_uint4(0u, 0u, 0u, 0u);
+        if (v >= 0) {
+            r0.x = pack_bf16(c0[v], c1[v]);
+            r0.y = pack_bf16(c2[v], 0.0f);
+        }
+        reinterpret_cast<uint4 *>(out + r * CH)[0] = r0;
+        reinterpret_cast<uint4 *>(out + r * CH)[1] = make_uint4(0u, 0u, 0u, 0u);
     }
 }
 
-// Loss 0.5 * mean (pred - target)^2 (FP64 partials) and its gradient,
-// scaled by `gscale`, into channel 0 of a BF16 [V][16] buffer.
-__global__ void mse_kernel(long long V, const float *__restrict__ pred, const float *__restrict__ target,
+// Loss 0.5 * mean (pred - target)^2 (FP64 partials) and its gradient, scaled
+// by `gscale`, into channel 0 of BF16 rows (zero halo).
+__global__ void mse_kernel(Geo g, const float *__restrict__ pred, const float *__restrict__ target,
                            float gscale, __nv_bfloat16 *__restrict__ grad, double *__restrict__ partial)
 {
     __shared__ double red[8];
     double acc = 0.0;
-    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < V; v += (long long)gridDim.x * blockDim.x) {
-        const float d = pred[v] - target[v];
-        acc += (double)d * d;
-        uint4 r0;
-        r0.x = pack_bf16(d * gscale, 0.0f);
-        r0.y = r0.z = r0.w = 0u;
-        reinterpret_cast<uint4 *>(grad + v * CH)[0] = r0;
-        reinterpret_cast<uint4 *>(grad + v * CH)[1] = make_uint4(0u, 0u, 0u, 0u);
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < g.R; r += (long long)gridDim.x * blockDim.x) {
+        const long long v = interior_of(g, r);
+        uint4 r0 = make_uint4(0u, 0u, 0u, 0u);
+        if (v >= 0) {
+            const float d = pred[v] - target[v];
+            acc += (double)d * d;
+            r0.x = pack_bf16(d * gscale, 0.0f);
+        }
+        reinterpret_cast<uint4 *>(grad + r * CH)[0] = r0;
+        reinterpret_cast<uint4 *>(grad + r * CH)[1] = make_uint4(0u, 0u, 0u, 0u);
     }
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
@@ -289,13 +652,14 @@ __global__ void mse_kernel(long long V, const float *__restrict__ pred, const fl
     }
 }
 
+// One warp: lane l sums p[l], p[l+32], ... in order, then a fixed shuffle tree.
 __global__ void sum_f64_kernel(const double *__restrict__ p, int n, double *__restrict__ out)
 {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double s = 0.0;
-        for (int i = 0; i < n; ++i) s += p[i];
-        *out = s;
-    }
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += 32) s += p[i];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) *out = s;
 }
 
 // Adam on the FP32 master weights (Kingma & Ba, 2015), then the BF16 copies:
@@ -384,43 +748,147 @@ namespace {
         }                                                                       \
     } while (0)
 
-int conv_blocks(const Geo &g)
+// Rows map over a padded BF16 activation buffer, seen as (8 channels, row,
+// channel half) with strides (2 B, 32 B, 16 B): an (8, 128, 2) box lands in
+// shared memory as two planes [half][row][8], the no-swizzle K-major operand
+// layout, and rows outside [0, R) read as zeros.
+int rows_map(fwi_cnn *n, const __nv_bfloat16 *base, int box_rows, CUtensorMap *m)
 {
-    const long long tiles = (long long)((g.nz + 15) / 16) * g.nx * g.ny;
-    long long b = (tiles + WARPS - 1) / WARPS;
-    return (int)std::min<long long>(std::max<long long>(b, 1), 148LL * 8);
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        CNN_CK(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !p) {
+            n->err = "cuTensorMapEncodeTiled unavailable";
+            return FWI_ERR_CUDA;
+        }
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    cuuint64_t dims[3] = {8, (cuuint64_t)n->g.R, 2};
+    cuuint64_t strides[2] = {CH * 2, 16};
+    cuuint32_t box[3] = {8, (cuuint32_t)box_rows, 2};
+    cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, (void *)base, dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        n->err = "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")";
+        return FWI_ERR_CUDA;
+    }
+    return FWI_OK;
+}
+
+// CTAs of a persistent tensor-core kernel that are resident at once: per SM
+// the fewest of `want`, what shared memory holds and what tensor memory (512
+// columns) holds.
+int resident_ctas(fwi_cnn *n, int smem_bytes, uint32_t tmem_cols, int want)
+{
+    int dev = 0, sms = 0, smem_sm = 0, reserved = 0;
+    CNN_CK(cudaGetDevice(&dev));
+    CNN_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CNN_CK(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    CNN_CK(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+    int per_sm = std::min(want, smem_sm / (smem_bytes + reserved));
+    per_sm = std::min(per_sm, (int)(512u / tmem_cols));
+    return sms * std::max(per_sm, 1);
+}
+
+template <int SIGN, int MODE>
+int launch_conv(fwi_cnn *n, const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias,
+                const __nv_bfloat16 *mask, __nv_bfloat16 *out, float *out32)
+{
+    static int ctas = 0;  // resident CTAs on the whole GPU
+    if (!ctas) {
+        CNN_CK(cudaFuncSetAttribute(conv_tc_kernel<SIGN, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    tc::SMEM));
+        // the whole unified L1 as shared memory, so that four CTAs fit
+        CNN_CK(cudaFuncSetAttribute(conv_tc_kernel<SIGN, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    (int)cudaSharedmemCarveoutMaxShared));
+        ctas = resident_ctas(n, tc::SMEM, tc::TMEM_COLS, tc::CTAS_PER_SM);
+        if (ctas <= 0) return FWI_ERR_CUDA;
+    }
+    CUtensorMap m;
+    const int st = rows_map(n, in, tc::BM, &m);
+    if (st != FWI_OK) return st;
+    ConvArgs a{n->g, (int)((n->g.R + tc::TM - 1) / tc::TM), w, bias, mask, out, out32};
+    const int blocks = std::max(1, std::min(a.ntiles, ctas));
+    conv_tc_kernel<SIGN, MODE><<<blocks, tc::THREADS, tc::SMEM, n->stream>>>(m, a);
+    CNN_CK(cudaGetLastError());
+    return FWI_OK;
 }
 
 int forward_impl(fwi_cnn *n)
 {
-    const Geo &g = n->g;
-    const int blocks = conv_blocks(g);
     for (int l = 0; l < NL; ++l) {
-        if (l < NL - 1) {
-            conv_kernel<1, 0><<<blocks, WARPS * 32, 0, n->stream>>>(g, n->act[l].p, n->wb[l].p, n->b32[l].p, nullptr,
-                                                                    n->act[l + 1].p, nullptr);
-        } else {
-            conv_kernel<1, 2><<<blocks, WARPS * 32, 0, n->stream>>>(g, n->act[l].p, n->wb[l].p, n->b32[l].p, nullptr,
-                                                                    nullptr, n->pred.p);
-        }
+        const int st = l < NL - 1
+                           ? launch_conv<1, 0>(n, n->act[l].p, n->wb[l].p, n->b32[l].p, nullptr, n->act[l + 1].p,
+                                               nullptr)
+                           : launch_conv<1, 2>(n, n->act[l].p, n->wb[l].p, n->b32[l].p, nullptr, nullptr,
+                                               n->pred.p);
+        if (st != FWI_OK) return st;
     }
+    return FWI_OK;
+}
+
+// Weight and bias gradients of one layer into gw / gb: x = the layer's input
+// rows, dy = the gradient rows of its output.
+int launch_wgrad(fwi_cnn *n, const __nv_bfloat16 *x, const __nv_bfloat16 *dy, float *gw, float *gb)
+{
+    static int ctas = 0;
+    if (!ctas) {
+        CNN_CK(cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, wg::SMEM));
+        CNN_CK(cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    (int)cudaSharedmemCarveoutMaxShared));
+        ctas = std::min(resident_ctas(n, wg::SMEM, wg::TMEM_COLS, wg::CTAS_PER_SM), kMaxPartials);
+    }
+    CUtensorMap mx, mdy;
+    int st = rows_map(n, x, wg::BK, &mx);
+    if (st == FWI_OK) st = rows_map(n, dy, wg::BROWS, &mdy);
+    if (st != FWI_OK) return st;
+    WgradArgs a{n->g, (int)((n->g.R + wg::BK - 1) / wg::BK), 0, n->partial.p, n->bpartial.p};
+    a.kb_per_cta = (a.nkb + ctas - 1) / ctas;
+    const int grid = (a.nkb + a.kb_per_cta - 1) / a.kb_per_cta;
+    wgrad_tc_kernel<<<grid, wg::THREADS, wg::SMEM, n->stream>>>(mx, mdy, a);
     CNN_CK(cudaGetLastError());
+    reduce_partials_kernel<<<(WSZ + RED_X - 1) / RED_X, RED_X * RED_Y, 0, n->stream>>>(n->partial.p, grid, WSZ, gw);
+    reduce_partials_kernel<<<1, RED_X * RED_Y, 0, n->stream>>>(n->bpartial.p, grid, CH, gb);
+    CNN_CK(cudaGetLastError());
+    return FWI_OK;
+}
+
+// After a synchronised run: a bounded wait that gave up in a tensor-core
+// kernel becomes FWI_ERR_TIMEOUT (and the flag is cleared).
+int check_cnn_status(fwi_cnn *n)
+{
+    unsigned st = 0;
+    CNN_CK(cudaMemcpyFromSymbol(&st, g_cnn_status, sizeof st));
+    if (st) {
+        const unsigned z = 0;
+        CNN_CK(cudaMemcpyToSymbol(g_cnn_status, &z, sizeof z));
+        n->err = st & 2u ? "convolution kernel: shared memory not 128-byte aligned"
+                         : "convolution kernel: a bounded wait gave up";
+        return st & 2u ? FWI_ERR_CUDA : FWI_ERR_TIMEOUT;
+    }
     return FWI_OK;
 }
 
 int ensure_volume(fwi_cnn *n, int nz, int nx, int ny)
 {
     if (nz < 1 || nx < 1 || ny < 1) return FWI_ERR_ARG;
-    n->g = Geo{nz, nx, ny, (long long)nz * nx * ny};
-    const size_t V = n->g.V;
-    for (int l = 0; l < NL; ++l) CNN_CK(n->act[l].ensure(V * CH));
-    for (int k = 0; k < 2; ++k) CNN_CK(n->dg[k].ensure(V * CH));
-    CNN_CK(n->pred.ensure(V));
-    const long long ncols = (long long)nx * ny;
-    const int cpc = (int)std::max<long long>(1, (ncols + 2047) / 2048);
-    const int nblk = (int)((ncols + cpc - 1) / cpc);
-    CNN_CK(n->partial.ensure((size_t)nblk * WSZ));
-    CNN_CK(n->bpartial.ensure((size_t)nblk * CH));
+    Geo g{nz, nx, ny, (long long)nz * nx * ny, nz + 2, nx + 2, (long long)(nz + 2) * (nx + 2) * (ny + 2),
+          make_fastdiv((uint32_t)(nz + 2)), make_fastdiv((uint32_t)(nx + 2))};
+    // TMA row coordinates are 32-bit
+    if (g.R + (long long)g.NZ2 * g.NX2 + 2 * tc::BM >= 0x7FFFFFFFLL) {
+        n->err = "volume too large for the convolution kernels";
+        return FWI_ERR_ARG;
+    }
+    n->g = g;
+    for (int l = 0; l < NL; ++l) CNN_CK(n->act[l].ensure(g.R * CH));
+    for (int k = 0; k < 2; ++k) CNN_CK(n->dg[k].ensure(g.R * CH));
+    CNN_CK(n->pred.ensure(g.V));
+    CNN_CK(n->partial.ensure((size_t)kMaxPartials * WSZ));
+    CNN_CK(n->bpartial.ensure((size_t)kMaxPartials * CH));
     CNN_CK(n->lpart.ensure(1024));
     CNN_CK(n->lsum.ensure(1));
     return FWI_OK;
@@ -566,12 +1034,12 @@ int fwi_cnn_forward(fwi_cnn *n, int nz, int nx, int ny, const float *d_in, float
     int st = ensure_volume(n, nz, nx, ny);
     if (st != FWI_OK) return st;
     const long long V = n->g.V;
-    pack_input_kernel<<<1184, 256, 0, n->stream>>>(V, d_in, d_in + V, d_in + 2 * V, n->act[0].p);
+    pack_input_kernel<<<1184, 256, 0, n->stream>>>(n->g, d_in, d_in + V, d_in + 2 * V, n->act[0].p);
     st = forward_impl(n);
     if (st != FWI_OK) return st;
     CNN_CK(cudaMemcpyAsync(d_out, n->pred.p, V * sizeof(float), cudaMemcpyDeviceToDevice, n->stream));
     CNN_CK(cudaStreamSynchronize(n->stream));
-    return FWI_OK;
+    return check_cnn_status(n);
 }
 
 // Gradients of the loss 0.5 mean (f(x) - target)^2 w.r.t. every weight and
@@ -585,29 +1053,23 @@ int fwi_cnn_train_step(fwi_cnn *n, int nz, int nx, int ny, const float *d_in, co
     if (st != FWI_OK) return st;
     const Geo &g = n->g;
     const long long V = g.V;
-    pack_input_kernel<<<1184, 256, 0, n->stream>>>(V, d_in, d_in + V, d_in + 2 * V, n->act[0].p);
+    pack_input_kernel<<<1184, 256, 0, n->stream>>>(g, d_in, d_in + V, d_in + 2 * V, n->act[0].p);
     st = forward_impl(n);
     if (st != FWI_OK) return st;
     // loss gradient d(0.5 mean d^2)/dpred = d / V, carried in BF16 scaled up
     // by V (loss scaling) and scaled back in the weight gradients
     const int lblk = 1024;
-    mse_kernel<<<lblk, 256, 0, n->stream>>>(V, n->pred.p, d_target, 1.0f, n->dg[0].p, n->lpart.p);
+    mse_kernel<<<lblk, 256, 0, n->stream>>>(g, n->pred.p, d_target, 1.0f, n->dg[0].p, n->lpart.p);
     sum_f64_kernel<<<1, 32, 0, n->stream>>>(n->lpart.p, lblk, n->lsum.p);
-    const long long ncols = (long long)g.nx * g.ny;
-    const int cpc = (int)std::max<long long>(1, (ncols + 2047) / 2048);
-    const int nblk = (int)((ncols + cpc - 1) / cpc);
-    const int blocks = conv_blocks(g);
     int cur = 0;
     for (int l = NL - 1; l >= 0; --l) {
         // weight and bias gradients of layer l: input act[l], output gradient dg[cur]
-        conv_wgrad_kernel<<<nblk, WG_WARPS * 32, 0, n->stream>>>(g, n->act[l].p, n->dg[cur].p, cpc, n->partial.p,
-                                                                  n->bpartial.p);
-        reduce_partials_kernel<<<(WSZ + 255) / 256, 256, 0, n->stream>>>(n->partial.p, nblk, WSZ, n->gw[l].p);
-        reduce_partials_kernel<<<1, 32, 0, n->stream>>>(n->bpartial.p, nblk, CH, n->gb[l].p);
+        st = launch_wgrad(n, n->act[l].p, n->dg[cur].p, n->gw[l].p, n->gb[l].p);
+        if (st != FWI_OK) return st;
         if (l > 0) {
             // data gradient through layer l, masked by the ReLU of act[l]
-            conv_kernel<-1, 1><<<blocks, WARPS * 32, 0, n->stream>>>(g, n->dg[cur].p, n->wt[l].p, nullptr,
-                                                                     n->act[l].p, n->dg[1 - cur].p, nullptr);
+            st = launch_conv<-1, 1>(n, n->dg[cur].p, n->wt[l].p, nullptr, n->act[l].p, n->dg[1 - cur].p, nullptr);
+            if (st != FWI_OK) return st;
             cur = 1 - cur;
         }
     }
@@ -615,6 +1077,8 @@ int fwi_cnn_train_step(fwi_cnn *n, int nz, int nx, int ny, const float *d_in, co
     double lsum = 0.0;
     CNN_CK(cudaMemcpyAsync(&lsum, n->lsum.p, sizeof(double), cudaMemcpyDeviceToHost, n->stream));
     CNN_CK(cudaStreamSynchronize(n->stream));
+    st = check_cnn_status(n);
+    if (st != FWI_OK) return st;
     if (loss) *loss = 0.5 * lsum / (double)V;
     // the loss gradient was d (not d/V): scale the parameter gradients by 1/V
     const float inv = 1.0f / (float)V;
