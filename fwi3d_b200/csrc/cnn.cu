@@ -125,8 +125,7 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 namespace tc {
 constexpr int BM = 128;                       // input rows per block (MMA M)
 constexpr int TM = BM - 2;                    // output rows per tile
-constexpr int PLANE = BM * 16;                // bytes of one 8-channel half of a block
-constexpr int SLOT = 2 * PLANE;
+constexpr int SLOT = BM * CH * 2;             // one block: 128 swizzled 32-byte rows
 constexpr int NS = 9;                         // ring slots (a tile takes 9)
 constexpr int NG = 3 * CH;                    // MMA N: (z tap, channel)
 constexpr int BJ = NG * CH * 2;               // bytes of the B operand of one (dx, dy)
@@ -236,7 +235,7 @@ __global__ void __launch_bounds__(tc::THREADS, tc::CTAS_PER_SM)
                     }
                     mbar_expect_tx(&full[slot], LOAD_BYTES);
                     const long long start = r0 + SIGN * (dx * (long long)a.g.NZ2 + dy * plane_xy) - 1;
-                    fwi::tma_load_3d(ring + slot * SLOT, &map, &full[slot], 0, (int)start, 0);
+                    fwi::tma_load_2d(ring + slot * SLOT, &map, &full[slot], 0, (int)start);
                     used |= 1u << slot;
                     phases = (phases & ~(1u << slot)) | (ph << slot);
                     if (++slot == NS) {
@@ -273,7 +272,7 @@ __global__ void __launch_bounds__(tc::THREADS, tc::CTAS_PER_SM)
                         break;
                     }
                     fwi::tc_fence_after();
-                    const uint64_t ad = fwi::umma_desc(ring_a + slot * SLOT, PLANE, 128);
+                    const uint64_t ad = fwi::umma_desc(ring_a + slot * SLOT, 16, 256, fwi::kSwizzle32B);
                     const uint64_t bd = fwi::umma_desc(w_a + j * BJ, NG * 16, 128);
                     fwi::umma_bf16(d, ad, bd, IDESC, j > 0 ? 1u : 0u);
                     fwi::umma_commit(&empty[slot]);
@@ -390,38 +389,35 @@ __global__ void __launch_bounds__(tc::THREADS, tc::CTAS_PER_SM)
 //                 = sum_u dy[u - dz][co] x[u + NZ2 dx + NZ2 NX2 dy][ci]   (u = v + dz)
 // over every padded row (halo rows of dy are zero).  Each CTA owns a range of
 // 128-row blocks of u.  Per block, TMA brings the x rows of the nine (dx, dy)
-// offsets and the dy rows u-1 .. u+130; both operands are MN-major (channels
-// contiguous), no swizzle.
-//   - Group 1: the x blocks of offsets 0..7 stacked along M (M = 8 x 16 ci).
-//   - Group 2: the x block of offset 8, then a block of ones in channel 0
+// offsets and the dy rows shifted by dz = -1, 0, +1, all as 32-byte-swizzled
+// rows: MN-major operands whose K is the row.
+//   - A, group 1: the x blocks of offsets 0..7 stacked along M (8 x 16 ci).
+//   - A, group 2: the x block of offset 8, then a block of ones in channel 0
 //     (M rows 16..31), then six blocks of group 1 whose rows are not used.
-//     Row 16 with dz = 0 is sum_u dy[u][co]: the bias gradient.
-// The z tap is the dy descriptor's start row (dz = -1, 0, 1 -> rows +2, +1,
-// +0), so each 16-row K step is six MMAs (M = 128, N = 16, K = 16) into six
+//     Row 16 against the dz = 0 columns is sum_u dy[u][co]: the bias gradient.
+//   - B: the three dy blocks side by side along N (N = 3 x 16 co).
+// Each 16-row K step is two MMAs (M = 128, N = 48, K = 16) into two
 // accumulators that live in tensor memory for the whole row range.  The
 // epilogue writes per-CTA partials [cta][27][16 co][16 ci] and [cta][16],
 // summed in a fixed order by reduce_partials_kernel.
 // ---------------------------------------------------------------------------
 namespace wg {
 constexpr int BK = 128;                        // rows of u per block (K)
-constexpr int APLANE = BK * 16;                // one channel half of an x block
-constexpr int ABLK = 2 * APLANE;
-constexpr int BROWS = BK + 4;                  // dy rows u-1 .. u+130
-constexpr int BPLANE = BROWS * 16;
-constexpr int BBLK = 2 * BPLANE;
-constexpr int OFF_B8 = 0, OFF_ONES = ABLK, OFF_G1 = 2 * ABLK, OFF_DY = 10 * ABLK;
-constexpr int STAGE = 10 * ABLK + BBLK;
+constexpr int BLK = BK * CH * 2;               // one block: 128 swizzled 32-byte rows
+// stage: [x block 8][ones][x blocks 0..7][dy blocks dz = -1, 0, +1]
+constexpr int OFF_B8 = 0, OFF_ONES = BLK, OFF_G1 = 2 * BLK, OFF_DY = 10 * BLK;
+constexpr int STAGE = 13 * BLK;
 constexpr int NSTAGE = 2;
 constexpr int THREADS = 192;
 constexpr int CTAS_PER_SM = 2;
-constexpr int NACC = 6;                        // 2 groups x 3 z taps
-constexpr uint32_t TMEM_COLS = 128;
-constexpr uint32_t LOAD_BYTES = 9 * ABLK + BBLK;
+constexpr int NG = 3 * CH;                     // MMA N: (z tap, c_out)
+constexpr uint32_t TMEM_COLS = 128;            // two 48-column accumulators
+constexpr uint32_t LOAD_BYTES = 12 * BLK;
 constexpr int BAR_BYTES = (2 * NSTAGE + 1) * 8;
 constexpr int SMEM = NSTAGE * STAGE + BAR_BYTES + 16;
-constexpr uint32_t IDESC = fwi::umma_idesc_bf16(128, CH, true, true);
-static_assert(STAGE % 128 == 0, "TMA destinations need 128-byte alignment");
-static_assert(NACC * CH <= (int)TMEM_COLS, "accumulator columns");
+constexpr uint32_t IDESC = fwi::umma_idesc_bf16(128, NG, true, true);
+static_assert(STAGE % 1024 == 0, "stage alignment");
+static_assert(2 * NG <= (int)TMEM_COLS, "accumulator columns");
 }  // namespace wg
 
 struct WgradArgs {
@@ -458,12 +454,13 @@ __global__ void __launch_bounds__(wg::THREADS, wg::CTAS_PER_SM)
         *abort_flag = 0;
         fwi::fence_mbar_init();
     }
-    // the ones block of every stage: channel 0 = 1 in every row (MN-major:
-    // plane 0 holds channels 0..7 of rows 0..127, 16 bytes per row)
-    for (int i = threadIdx.x; i < NSTAGE * ABLK / 16; i += blockDim.x) {
-        const int st = i / (ABLK / 16), k = i % (ABLK / 16);
-        const uint4 one = make_uint4(k < BK ? 0x3F80u : 0u, 0u, 0u, 0u);  // BF16 1.0 in the low half
-        *reinterpret_cast<uint4 *>(smem + st * STAGE + OFF_ONES + k * 16) = one;
+    // the ones block of every stage: channel 0 = 1 in every row.  In the
+    // 32-byte swizzle, the 16-byte half h of row r sits at half h ^ (r/4 % 2).
+    for (int i = threadIdx.x; i < NSTAGE * BK * 2; i += blockDim.x) {
+        const int st = i / (BK * 2), r = (i >> 1) % BK, h = i & 1;
+        const int logical = h ^ ((r >> 2) & 1);
+        const uint4 v = make_uint4(logical == 0 ? 0x3F80u : 0u, 0u, 0u, 0u);  // BF16 1.0 in channel 0
+        *reinterpret_cast<uint4 *>(smem + st * STAGE + OFF_ONES + r * 32 + h * 16) = v;
     }
     fwi::fence_proxy_async();
     if (warp == 1) fwi::tmem_alloc(tmem_slot, TMEM_COLS);
@@ -493,9 +490,10 @@ __global__ void __launch_bounds__(wg::THREADS, wg::CTAS_PER_SM)
                 for (int j = 0; j < 9; ++j) {
                     const int dx = j % 3 - 1, dy = j / 3 - 1;
                     const long long r = u0 + dx * (long long)a.g.NZ2 + dy * plane_xy;
-                    fwi::tma_load_3d(base + (j < 8 ? OFF_G1 + j * ABLK : OFF_B8), &mx, &full[st], 0, (int)r, 0);
+                    fwi::tma_load_2d(base + (j < 8 ? OFF_G1 + j * BLK : OFF_B8), &mx, &full[st], 0, (int)r);
                 }
-                fwi::tma_load_3d(base + OFF_DY, &mdy, &full[st], 0, (int)(u0 - 1), 0);
+                for (int k = 0; k < 3; ++k)  // dy rows u - dz, dz = k - 1
+                    fwi::tma_load_2d(base + OFF_DY + k * BLK, &mdy, &full[st], 0, (int)(u0 - (k - 1)));
                 used |= 1u << st;
                 phases = (phases & ~(1u << st)) | (ph << st);
                 if (++st == NSTAGE) {
@@ -522,16 +520,13 @@ __global__ void __launch_bounds__(wg::THREADS, wg::CTAS_PER_SM)
                 const uint32_t base = s_a + st * STAGE;
 #pragma unroll 1
                 for (int s = 0; s < BK / 16; ++s) {
-                    const uint32_t koff = s * 256;  // 16 rows = two 8-row K groups
+                    const uint32_t koff = s * 512;  // 16 rows of 32 bytes
+                    const uint64_t bd = fwi::umma_desc(base + OFF_DY + koff, BLK, 256, fwi::kSwizzle32B);
 #pragma unroll
                     for (int g = 0; g < 2; ++g) {
-                        const uint64_t ad = fwi::umma_desc(base + (g ? OFF_B8 : OFF_G1) + koff, 128, APLANE);
-#pragma unroll
-                        for (int dz = -1; dz <= 1; ++dz) {
-                            const uint64_t bd = fwi::umma_desc(base + OFF_DY + (1 - dz) * 16 + koff, 128, BPLANE);
-                            fwi::umma_bf16(tmem + (uint32_t)(3 * g + dz + 1) * CH, ad, bd, IDESC,
-                                           (first && s == 0) ? 0u : 1u);
-                        }
+                        const uint64_t ad =
+                            fwi::umma_desc(base + (g ? OFF_B8 : OFF_G1) + koff, BLK, 256, fwi::kSwizzle32B);
+                        fwi::umma_bf16(tmem + (uint32_t)(g * NG), ad, bd, IDESC, (first && s == 0) ? 0u : 1u);
                     }
                 }
                 first = false;
@@ -553,7 +548,8 @@ __global__ void __launch_bounds__(wg::THREADS, wg::CTAS_PER_SM)
             const int m = 32 * q + lane;  // accumulator row
             float *P = a.partial + (long long)blockIdx.x * WSZ;
 #pragma unroll 1
-            for (int acc = 0; acc < NACC; ++acc) {
+            for (int acc = 0; acc < 6; ++acc) {
+                // accumulator g = acc / 3, columns of z tap dz = acc % 3 - 1
                 uint32_t v[16];
                 fwi::tmem_ld16(tmem + (uint32_t)acc * CH + ((uint32_t)(32 * q) << 16), v);
                 fwi::tmem_wait_ld();
@@ -748,10 +744,9 @@ namespace {
         }                                                                       \
     } while (0)
 
-// Rows map over a padded BF16 activation buffer, seen as (8 channels, row,
-// channel half) with strides (2 B, 32 B, 16 B): an (8, 128, 2) box lands in
-// shared memory as two planes [half][row][8], the no-swizzle K-major operand
-// layout, and rows outside [0, R) read as zeros.
+// Rows map over a padded BF16 activation buffer: (16 channels, row), box of
+// `box_rows` whole 32-byte rows, 32-byte swizzle (the SW32 operand layout of
+// the tensor-core descriptors).  Rows outside [0, R) read as zeros.
 int rows_map(fwi_cnn *n, const __nv_bfloat16 *base, int box_rows, CUtensorMap *m)
 {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -765,12 +760,12 @@ int rows_map(fwi_cnn *n, const __nv_bfloat16 *base, int box_rows, CUtensorMap *m
         }
         fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
     }
-    cuuint64_t dims[3] = {8, (cuuint64_t)n->g.R, 2};
-    cuuint64_t strides[2] = {CH * 2, 16};
-    cuuint32_t box[3] = {8, (cuuint32_t)box_rows, 2};
-    cuuint32_t estr[3] = {1, 1, 1};
-    const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, (void *)base, dims, strides, box, estr,
-                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+    cuuint64_t dims[2] = {CH, (cuuint64_t)n->g.R};
+    cuuint64_t strides[1] = {CH * 2};
+    cuuint32_t box[2] = {CH, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void *)base, dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         n->err = "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")";
@@ -844,7 +839,7 @@ int launch_wgrad(fwi_cnn *n, const __nv_bfloat16 *x, const __nv_bfloat16 *dy, fl
     }
     CUtensorMap mx, mdy;
     int st = rows_map(n, x, wg::BK, &mx);
-    if (st == FWI_OK) st = rows_map(n, dy, wg::BROWS, &mdy);
+    if (st == FWI_OK) st = rows_map(n, dy, wg::BK, &mdy);
     if (st != FWI_OK) return st;
     WgradArgs a{n->g, (int)((n->g.R + wg::BK - 1) / wg::BK), 0, n->partial.p, n->bpartial.p};
     a.kb_per_cta = (a.nkb + ctas - 1) / ctas;

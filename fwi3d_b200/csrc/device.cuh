@@ -162,6 +162,16 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
         : "memory");
 }
 
+// 2-D tiled TMA load, completing on bar.  No multicast.
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0, int c1)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_addr(bar)), "r"(c0), "r"(c1)
+        : "memory");
+}
+
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
 {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
@@ -187,16 +197,24 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols)
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// Shared-memory matrix descriptor, no swizzle.  Core matrices are 128
-// contiguous bytes.  K-major: 8 M/N rows x 16 bytes of K; lbo = byte stride
-// between K halves, sbo = byte stride between 8-row groups.  MN-major: 8 K
-// rows x 16 bytes of M/N; lbo = byte stride between 8-row K groups, sbo =
-// byte stride between 8-element M/N groups.  Bit 46 is the tcgen05
-// descriptor version.
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+// Shared-memory matrix descriptor.  Bit 46 is the tcgen05 descriptor version.
+// No swizzle: core matrices are 128 contiguous bytes.  K-major: 8 M/N rows x
+// 16 bytes of K; lbo = byte stride between K halves, sbo = byte stride
+// between 8-row groups.  MN-major: 8 K rows x 16 bytes of M/N; lbo = byte
+// stride between 8-row K groups, sbo = byte stride between 8-element M/N
+// groups.
+// 32-byte swizzle (the pattern a SWIZZLE_32B TMA load writes: the 16-byte
+// half of each 32-byte row flips with address bit 7): rows of 32 bytes.
+// K-major (K = 16 BF16 per row): sbo = stride between 8-row groups, lbo
+// unused.  MN-major (16 M/N elements per row, K along rows): lbo = stride
+// between 16-element M/N groups, sbo = stride between 8-row K groups.
+constexpr uint64_t kSwizzleNone = 0, kSwizzle32B = 6;  // layout type, bits 61..63
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo,
+                                              uint64_t layout = kSwizzleNone)
 {
     return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46) | (layout << 61);
 }
 
 // Instruction descriptor of kind::f16: D FP32, A and B BF16; a_mn / b_mn
