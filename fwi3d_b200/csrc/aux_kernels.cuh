@@ -143,6 +143,12 @@ __global__ void transpose_kernel(const float *__restrict__ in, long long rows, l
 // last depth sample 0 (Migration::export_seismic,
 // src/migration/migration.cu:137-164), FP32 like the reference.
 // ---------------------------------------------------------------------------
+// Image or gradient over illumination.  A cell the source field never
+// reached has illumination 0 and no image either; the reference's 0/0 there
+// is NaN (src/migration/migration.cu:100, src/inversion/inversion.cu:150), the
+// project defines it as 0.
+__device__ __forceinline__ float ratio(float a, float ill) { return ill != 0.0f ? a / ill : 0.0f; }
+
 __global__ void rtm_image_kernel(const float *__restrict__ img, const float *__restrict__ ill,
                                  int nz, int nx, int ny, int nb, int nxx, int ldz, float idh2,
                                  float *__restrict__ out)
@@ -156,9 +162,9 @@ __global__ void rtm_image_kernel(const float *__restrict__ img, const float *__r
         float v = 0.0f;
         if (i > 0 && i < nz - 1) {
             const long long p = (i + nb) + (long long)(j + nb) * ldz + (long long)(k + nb) * ldz * nxx;
-            const float sm = img[p - 1] / ill[p - 1];
-            const float s0 = img[p] / ill[p];
-            const float sp = img[p + 1] / ill[p + 1];
+            const float sm = ratio(img[p - 1], ill[p - 1]);
+            const float s0 = ratio(img[p], ill[p]);
+            const float sp = ratio(img[p + 1], ill[p + 1]);
             v = -1.0f * (sm - 2.0f * s0 + sp) * idh2;
         }
         out[c] = v;
@@ -183,9 +189,9 @@ __global__ void grad_post_kernel(const float *__restrict__ g, const float *__res
         float v = 0.0f;
         if (i > imask && i < nz - 1) {
             const long long p = (i + nb) + (long long)(j + nb) * ldz + (long long)(k + nb) * ldz * nxx;
-            const float sm = g[p - 1] / ill[p - 1];
-            const float s0 = g[p] / ill[p];
-            const float sp = g[p + 1] / ill[p + 1];
+            const float sm = ratio(g[p - 1], ill[p - 1]);
+            const float s0 = ratio(g[p], ill[p]);
+            const float sp = ratio(g[p + 1], ill[p + 1]);
             v = -1.0f * (sm - 2.0f * s0 + sp) * idh2;
         }
         out[c] = v;
@@ -199,7 +205,8 @@ __global__ void grad_post_kernel(const float *__restrict__ g, const float *__res
 __global__ void scale_by_inverse_kernel(float *__restrict__ g, long long n,
                                         const unsigned int *__restrict__ gmax_bits)
 {
-    const float s = 1.0f / __uint_as_float(*gmax_bits);
+    const float m = __uint_as_float(*gmax_bits);
+    const float s = m > 0.0f ? 1.0f / m : 0.0f;  // an all-zero gradient stays zero
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
          c += (long long)gridDim.x * blockDim.x)
         g[c] *= s;

@@ -359,7 +359,9 @@ void orc_rtm_post(const double *image_pad, const double *illum_pad, int nz, int 
     double *s = (double *)malloc(n * sizeof(double));
     orc_reduce(image_pad, nz, nx, ny, nb, a);
     orc_reduce(illum_pad, nz, nx, ny, nb, s);
-    for (size_t c = 0; c < n; ++c) s[c] = a[c] / s[c];
+    /* 0 where the illumination is 0: the reference's 0/0 is NaN there; the
+     * project defines it as 0 */
+    for (size_t c = 0; c < n; ++c) s[c] = s[c] != 0.0 ? a[c] / s[c] : 0.0;
     double idh2 = 1.0 / (dh * dh);
 #pragma omp parallel for
     for (long c = 0; c < (long)n; ++c) {
@@ -383,7 +385,7 @@ double orc_gradient_post(const double *grad_pad, const double *illum_pad, int nz
     double *s = (double *)malloc(n * sizeof(double));
     orc_reduce(grad_pad, nz, nx, ny, nb, g);
     orc_reduce(illum_pad, nz, nx, ny, nb, s);
-    for (size_t c = 0; c < n; ++c) s[c] = g[c] / s[c];
+    for (size_t c = 0; c < n; ++c) s[c] = s[c] != 0.0 ? g[c] / s[c] : 0.0;  /* as orc_rtm_post */
     double idh2 = 1.0 / (dh * dh);
     int imask = (int)(zmask / dh);
     double gmax = 0.0;
@@ -393,7 +395,8 @@ double orc_gradient_post(const double *grad_pad, const double *illum_pad, int nz
         out[c] = v;
         if (fabs(v) > gmax) gmax = fabs(v);
     }
-    for (size_t c = 0; c < n; ++c) out[c] *= 1.0 / gmax;
+    if (gmax > 0.0)
+        for (size_t c = 0; c < n; ++c) out[c] *= 1.0 / gmax;
     free(g);
     free(s);
     return gmax;
