@@ -105,48 +105,62 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 // of BF16 outputs are written as zeros, so every output is again a padded
 // input.
 //
-// A tile is 126 output rows r0..r0+125.  For each (dx, dy) one TMA load brings
-// the 128 input rows r0 + SIGN (dx NZ2 + dy NZ2 NX2) - 1 + i (i = 0..127), and
-// one MMA (M = 128 rows, N = 48, K = 16 channels) multiplies them by the
-// weights of the three z taps side by side: column group k holds z tap
-// dz = SIGN (k - 1), and group k of block row m + k feeds output row m:
-//     out[r0 + m] = D[m][group 0] + D[m+1][group 1] + D[m+2][group 2].
-// Nine MMAs per tile; the epilogue adds the three groups across rows (warp
-// shuffles, plus a small shared exchange for the two rows that cross a warp
-// boundary).
+// A tile is 120 output rows r0..r0+119, four warp segments of 30.  For each
+// (dx, dy) one 128-row MMA block (M = 128, N = 48, K = 16 channels) multiplies
+// input rows by the weights of the three z taps side by side: column group k
+// holds z tap dz = SIGN (k - 1).  Block row 32 q + i (q = 0..3, i = 0..31) is
+// input row r0 - 1 + 30 q + i + SIGN (dx NZ2 + dy NZ2 NX2): four 32-row TMA
+// segments that overlap by two rows, so that output row r0 + 30 q + j
+// (j < 30) only needs accumulator rows 32 q + j .. 32 q + j + 2, all in the
+// TMEM lanes of epilogue warp q:
+//     out = D[32q+j][group 0] + D[32q+j+1][group 1] + D[32q+j+2][group 2].
+// Nine MMAs per tile; the epilogue adds the three groups with warp shuffles.
+//
+// Tiles stream along y: tile (pos, k) covers rows pos*120 + k*P + m, P = NZ2
+// NX2 the rows of one y plane, m < 120 and pos*120 + m < P.  Its nine blocks
+// are three x offsets in each of the planes k-1, k, k+1, so a CTA walking k
+// upwards loads one new plane (three TMA copies) per tile and keeps the other
+// two in a ring of PS plane slots, like the stencil kernels' y queue.  Each
+// CTA owns a contiguous range of tiles in (pos, k) order; a run restarts the
+// plane stream where pos changes.
 //
 // Warp 0 issues the TMA loads, warp 1 allocates tensor memory and issues the
 // MMAs, warps 2..5 drain the accumulators (warp w reads TMEM lanes 32 (w%4)..).
 // Two accumulators alternate, so the epilogue of one tile overlaps the MMAs of
-// the next, and four CTAs share an SM's tensor pipe.  Every wait is bounded; a
-// wait that gives up sets g_cnn_status, and the kernel drains its copies and
+// the next, and three CTAs share an SM's tensor pipe.  Every wait is bounded;
+// a wait that gives up sets g_cnn_status, and the kernel drains its copies and
 // MMAs, frees its tensor memory and returns.
 // ---------------------------------------------------------------------------
 namespace tc {
-constexpr int BM = 128;                       // input rows per block (MMA M)
-constexpr int TM = BM - 2;                    // output rows per tile
-constexpr int SLOT = BM * CH * 2;             // one block: 128 swizzled 32-byte rows
-constexpr int NS = 9;                         // ring slots (a tile takes 9)
+constexpr int BM = 128;                       // rows per MMA block (M)
+constexpr int SEG = 32;                       // rows per TMA segment = TMEM lanes per epilogue warp
+constexpr int OSEG = SEG - 2;                 // output rows per segment
+constexpr int TM = 4 * OSEG;                  // output rows per tile
+constexpr int BLK = BM * CH * 2;              // one block: 128 swizzled 32-byte rows
+constexpr int PSLOT = 3 * BLK;                // one plane: blocks for x offsets -1, 0, +1
+constexpr int PS = 4;                         // plane slots (a tile reads 3)
 constexpr int NG = 3 * CH;                    // MMA N: (z tap, channel)
 constexpr int BJ = NG * CH * 2;               // bytes of the B operand of one (dx, dy)
 constexpr int WBYTES = 9 * BJ;
-constexpr int XBYTES = 2 * 4 * 2 * 32 * 4;    // [tile parity][warp][row][32 floats]
 constexpr int THREADS = 192;
-constexpr int CTAS_PER_SM = 4;                // registers: 4 x 192 threads x 80
+constexpr int CTAS_PER_SM = 3;
 constexpr uint32_t ACC_STRIDE = 64;           // TMEM columns between the two accumulators
 constexpr uint32_t TMEM_COLS = 128;
-constexpr uint32_t LOAD_BYTES = SLOT;
-constexpr int BAR_BYTES = (2 * NS + 5) * 8;
-constexpr int SMEM = NS * SLOT + WBYTES + XBYTES + BAR_BYTES + 16 + CH * 4;
+constexpr uint32_t LOAD_BYTES = PSLOT;
+constexpr int BAR_BYTES = (2 * PS + 5) * 8;
+constexpr int SMEM = PS * PSLOT + WBYTES + BAR_BYTES + 16 + CH * 4;
 constexpr uint32_t IDESC = fwi::umma_idesc_bf16(BM, NG);
-static_assert(NS < 32, "slot bitmasks");
-static_assert(BM <= 256, "TMA box dimension limit");
+static_assert(PS >= 4 && PS < 32, "plane slots");
+static_assert(4 * SEG == BM, "four segments per block");
 static_assert(NG <= (int)ACC_STRIDE, "accumulator columns");
 }  // namespace tc
 
 struct ConvArgs {
     Geo g;
-    int ntiles;
+    long long P;                // rows of one y plane, NZ2 * NX2
+    int ny2;                    // y planes, ny + 2
+    int ntiles;                 // tiles: ceil(P / 126) positions x ny2 planes
+    int tiles_per_cta;
     const __nv_bfloat16 *w;     // [27][16 n][16 k]: B operand rows n, K = k
     const float *bias;          // [16] (MODE 0, 2)
     const __nv_bfloat16 *mask;  // padded rows (MODE 1)
@@ -167,16 +181,15 @@ __global__ void __launch_bounds__(tc::THREADS, tc::CTAS_PER_SM)
     using namespace tc;
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char *ring = smem;
-    unsigned char *wsm = smem + NS * SLOT;
-    float *xch = reinterpret_cast<float *>(wsm + WBYTES);
-    uint64_t *full = reinterpret_cast<uint64_t *>(wsm + WBYTES + XBYTES);
-    uint64_t *empty = full + NS;
-    uint64_t *accf = empty + NS;  // [2] accumulator ready
+    unsigned char *wsm = smem + PS * PSLOT;
+    uint64_t *full = reinterpret_cast<uint64_t *>(wsm + WBYTES);
+    uint64_t *empty = full + PS;
+    uint64_t *accf = empty + PS;  // [2] accumulator ready
     uint64_t *acce = accf + 2;    // [2] accumulator drained
     uint64_t *done = acce + 2;    // every MMA of this CTA completed
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
-    float *bsm = reinterpret_cast<float *>(wsm + WBYTES + XBYTES + BAR_BYTES + 16);
+    float *bsm = reinterpret_cast<float *>(wsm + WBYTES + BAR_BYTES + 16);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if ((smem_addr(smem) & 127u) != 0u) {  // TMA destinations need 128-byte alignment
@@ -184,7 +197,7 @@ __global__ void __launch_bounds__(tc::THREADS, tc::CTAS_PER_SM)
         return;
     }
     if (threadIdx.x == 0) {
-        for (int s = 0; s < NS; ++s) {
+        for (int s = 0; s < PS; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
@@ -215,37 +228,44 @@ __global__ void __launch_bounds__(tc::THREADS, tc::CTAS_PER_SM)
     __syncthreads();
     fwi::tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    const long long plane_xy = (long long)a.g.NZ2 * a.g.NX2;
+    const int T0 = blockIdx.x * a.tiles_per_cta;
+    const int T1 = min(T0 + a.tiles_per_cta, a.ntiles);
 
     if (warp == 0) {
         if (lane == 0) {
-            // producer: one 128-row block per (dx, dy); rows outside the
-            // tensor read as zeros
+            // producer: plane k' of a run = three 128-row blocks at x offsets
+            // -1, 0, +1; rows outside the tensor read as zeros
             fwi::prefetch_tmap(&map);
             uint32_t used = 0, phases = 0;
-            int slot = 0;
-            uint32_t ph = 0;
-            for (long long tile = blockIdx.x; tile < a.ntiles && !*abort_flag; tile += gridDim.x) {
-                const long long r0 = tile * TM;
-                for (int j = 0; j < 9; ++j) {
-                    const int dx = j % 3 - 1, dy = j / 3 - 1;
-                    if (!mbar_wait(&empty[slot], ph ^ 1u)) {
+            unsigned g = 0;  // planes issued
+            bool stop = false;
+            for (int T = T0; T < T1 && !stop;) {
+                const int pos = T / a.ny2, ks = T % a.ny2;
+                const int te = min(T1, (pos + 1) * a.ny2);
+                const long long rb = (long long)pos * TM - 1;
+                for (int j = 0; j < te - T + 2; ++j, ++g) {
+                    const int slot = (int)(g % PS);
+                    const uint32_t ph = (g / PS) & 1u;
+                    if (*abort_flag || !mbar_wait(&empty[slot], ph ^ 1u)) {
                         cnn_fail(abort_flag);
+                        stop = true;
                         break;
                     }
                     mbar_expect_tx(&full[slot], LOAD_BYTES);
-                    const long long start = r0 + SIGN * (dx * (long long)a.g.NZ2 + dy * plane_xy) - 1;
-                    fwi::tma_load_2d(ring + slot * SLOT, &map, &full[slot], 0, (int)start);
+                    const long long r = rb + (long long)(ks - 1 + j) * a.P;
+#pragma unroll
+                    for (int bx = 0; bx < 3; ++bx)
+#pragma unroll
+                        for (int sg = 0; sg < 4; ++sg)
+                            fwi::tma_load_2d(ring + slot * PSLOT + bx * BLK + sg * SEG * CH * 2, &map, &full[slot],
+                                             0, (int)(r + (bx - 1) * (long long)a.g.NZ2 + sg * OSEG));
                     used |= 1u << slot;
                     phases = (phases & ~(1u << slot)) | (ph << slot);
-                    if (++slot == NS) {
-                        slot = 0;
-                        ph ^= 1u;
-                    }
                 }
+                T = te;
             }
             // no copy may land after the CTA has gone
-            for (int s = 0; s < NS; ++s)
+            for (int s = 0; s < PS; ++s)
                 if ((used >> s) & 1u)
                     if (!mbar_wait(&full[s], (phases >> s) & 1u)) atomicOr(&g_cnn_status, 1u);
         }
@@ -253,91 +273,86 @@ __global__ void __launch_bounds__(tc::THREADS, tc::CTAS_PER_SM)
         if (lane == 0) {
             // MMA issuer
             const uint32_t ring_a = smem_addr(ring), w_a = smem_addr(wsm);
-            int slot = 0;
-            uint32_t ph = 0;
+            unsigned g = 0;  // planes consumed
             int it = 0;
-            for (long long tile = blockIdx.x; tile < a.ntiles && !*abort_flag; tile += gridDim.x, ++it) {
-                const int buf = it & 1;
-                if (!mbar_wait(&acce[buf], (((uint32_t)it >> 1) & 1u) ^ 1u)) {
-                    cnn_fail(abort_flag);
-                    break;
-                }
-                fwi::tc_fence_after();
-                const uint32_t d = tmem + (uint32_t)buf * ACC_STRIDE;
-                bool ok = true;
-                for (int j = 0; j < 9; ++j) {
-                    if (!mbar_wait(&full[slot], ph)) {
+            bool stop = false;
+            for (int T = T0; T < T1 && !stop;) {
+                const int pos = T / a.ny2;
+                const int te = min(T1, (pos + 1) * a.ny2);
+                const int n = te - T;
+                for (int i = 0; i < n; ++i, ++it) {
+                    const int buf = it & 1;
+                    bool ok = !*abort_flag && mbar_wait(&acce[buf], (((uint32_t)it >> 1) & 1u) ^ 1u);
+                    // planes i, i+1, i+2 of the run (i, i+1 already waited unless i == 0)
+                    for (int jp = (i == 0 ? 0 : 2); ok && jp <= 2; ++jp) {
+                        const unsigned pl = g + i + jp;
+                        ok = mbar_wait(&full[pl % PS], (pl / PS) & 1u);
+                    }
+                    if (!ok) {
                         cnn_fail(abort_flag);
-                        ok = false;
+                        stop = true;
                         break;
                     }
                     fwi::tc_fence_after();
-                    const uint64_t ad = fwi::umma_desc(ring_a + slot * SLOT, 16, 256, fwi::kSwizzle32B);
-                    const uint64_t bd = fwi::umma_desc(w_a + j * BJ, NG * 16, 128);
-                    fwi::umma_bf16(d, ad, bd, IDESC, j > 0 ? 1u : 0u);
-                    fwi::umma_commit(&empty[slot]);
-                    if (++slot == NS) {
-                        slot = 0;
-                        ph ^= 1u;
+                    const uint32_t d = tmem + (uint32_t)buf * ACC_STRIDE;
+#pragma unroll
+                    for (int j = 0; j < 9; ++j) {
+                        const int dx = j % 3 - 1, dy = j / 3 - 1;
+                        const unsigned pl = g + i + 1 + SIGN * dy;
+                        const uint32_t blk = ring_a + (pl % PS) * PSLOT + (1 + SIGN * dx) * BLK;
+                        const uint64_t ad = fwi::umma_desc(blk, 16, 256, fwi::kSwizzle32B);
+                        const uint64_t bd = fwi::umma_desc(w_a + j * BJ, NG * 16, 128);
+                        fwi::umma_bf16(d, ad, bd, IDESC, j > 0 ? 1u : 0u);
+                    }
+                    fwi::umma_commit(&accf[buf]);
+                    // plane i is not read again; at the end of the run neither are i+1, i+2
+                    fwi::umma_commit(&empty[(g + i) % PS]);
+                    if (i == n - 1) {
+                        fwi::umma_commit(&empty[(g + i + 1) % PS]);
+                        fwi::umma_commit(&empty[(g + i + 2) % PS]);
                     }
                 }
-                if (!ok) break;
-                fwi::umma_commit(&accf[buf]);
+                g += n + 2;
+                T = te;
             }
             fwi::umma_commit(done);
             if (!mbar_wait(done, 0)) atomicOr(&g_cnn_status, 1u);
         }
     } else {
-        // epilogue: accumulator row 32 q + lane, q = warp % 4.  Every epilogue
-        // thread reaches the named barrier once per tile; its AND decides
-        // together whether all four warps go on (tcgen05.ld is
-        // warp-collective, bar.red is block-partial: both need uniform exits)
+        // epilogue: warp q drains TMEM lanes 32 q .. 32 q + 31 and writes
+        // output rows 30 q .. 30 q + 29 of the tile; waits and exits are
+        // warp-uniform (tcgen05.ld is warp-collective)
         const int q = warp & 3;
         int it = 0;
-        for (long long tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++it) {
+        for (int T = T0; T < T1; ++T, ++it) {
             const int buf = it & 1;
             bool ok = *abort_flag == 0 && mbar_wait(&accf[buf], ((uint32_t)it >> 1) & 1u);
-            ok = __all_sync(0xffffffffu, ok);
-            uint32_t v0[16], v1[16], v2[16];
-            float *xb = xch + (it & 1) * (4 * 2 * 32);
-            if (ok) {
-                fwi::tc_fence_after();
-                const uint32_t t0 = tmem + (uint32_t)buf * ACC_STRIDE + ((uint32_t)(32 * q) << 16);
-                fwi::tmem_ld16(t0, v0);
-                fwi::tmem_ld16(t0 + CH, v1);
-                fwi::tmem_ld16(t0 + 2 * CH, v2);
-                fwi::tmem_wait_ld();
-                fwi::tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&acce[buf]);
-                // rows 32q and 32q+1 also feed the two last rows of warp q-1
-                if (q >= 1 && lane < 2) {
-#pragma unroll
-                    for (int c = 0; c < CH; ++c) {
-                        xb[(q * 2 + lane) * 32 + c] = __uint_as_float(v1[c]);
-                        xb[(q * 2 + lane) * 32 + CH + c] = __uint_as_float(v2[c]);
-                    }
-                }
-            }
-            if (!fwi::bar_and(1, 128, ok)) {
-                if (lane == 0 && ok) cnn_fail(abort_flag);
+            if (!__all_sync(0xffffffffu, ok)) {
+                if (lane == 0) cnn_fail(abort_flag);
                 break;
             }
-            // output row m = D[m][0:16] + D[m+1][16:32] + D[m+2][32:48]
-            const int m = 32 * q + lane;
+            fwi::tc_fence_after();
+            uint32_t v0[16], v1[16], v2[16];
+            const uint32_t t0 = tmem + (uint32_t)buf * ACC_STRIDE + ((uint32_t)(32 * q) << 16);
+            fwi::tmem_ld16(t0, v0);
+            fwi::tmem_ld16(t0 + CH, v1);
+            fwi::tmem_ld16(t0 + 2 * CH, v2);
+            fwi::tmem_wait_ld();
+            fwi::tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acce[buf]);
+            // output row j = lane: group 0 of lane j, group 1 of lane j+1, group 2 of lane j+2
             float o[CH];
 #pragma unroll
             for (int c = 0; c < CH; ++c) {
-                float b1 = __shfl_down_sync(0xffffffffu, __uint_as_float(v1[c]), 1);
-                float b2 = __shfl_down_sync(0xffffffffu, __uint_as_float(v2[c]), 2);
-                if (q < 3) {
-                    if (lane == 31) b1 = xb[((q + 1) * 2) * 32 + c];
-                    if (lane >= 30) b2 = xb[((q + 1) * 2 + lane - 30) * 32 + CH + c];
-                }
+                const float b1 = __shfl_down_sync(0xffffffffu, __uint_as_float(v1[c]), 1);
+                const float b2 = __shfl_down_sync(0xffffffffu, __uint_as_float(v2[c]), 2);
                 o[c] = (__uint_as_float(v0[c]) + b1) + b2;
             }
-            const long long r = tile * TM + m;
-            if (m >= TM || r >= a.g.R) continue;
+            const int pos = T / a.ny2, k = T % a.ny2;
+            const long long zx = (long long)pos * TM + OSEG * q + lane;  // row within the y plane
+            if (lane >= OSEG || zx >= a.P) continue;
+            const long long r = zx + (long long)k * a.P;
             const long long vox = interior_of(a.g, r);
             if constexpr (MODE == 2) {
                 if (vox >= 0) a.out32[vox] = o[0] + bsm[0];
@@ -804,10 +819,14 @@ int launch_conv(fwi_cnn *n, const __nv_bfloat16 *in, const __nv_bfloat16 *w, con
         if (ctas <= 0) return FWI_ERR_CUDA;
     }
     CUtensorMap m;
-    const int st = rows_map(n, in, tc::BM, &m);
+    const int st = rows_map(n, in, tc::SEG, &m);
     if (st != FWI_OK) return st;
-    ConvArgs a{n->g, (int)((n->g.R + tc::TM - 1) / tc::TM), w, bias, mask, out, out32};
-    const int blocks = std::max(1, std::min(a.ntiles, ctas));
+    const long long P = (long long)n->g.NZ2 * n->g.NX2;
+    const int ny2 = n->g.ny + 2;
+    const int ntiles = (int)((P + tc::TM - 1) / tc::TM) * ny2;
+    const int tpc = (ntiles + ctas - 1) / ctas;
+    ConvArgs a{n->g, P, ny2, ntiles, tpc, w, bias, mask, out, out32};
+    const int blocks = (ntiles + tpc - 1) / tpc;
     conv_tc_kernel<SIGN, MODE><<<blocks, tc::THREADS, tc::SMEM, n->stream>>>(m, a);
     CNN_CK(cudaGetLastError());
     return FWI_OK;
