@@ -7,6 +7,7 @@ fwi_cnn_* in libfwi3d.so (BF16 tensor cores, FP32 accumulation, FP32 Adam).
 
     python -m fwi3d_b200.precond pipeline --models 0:136 --weights W.npz --report R.json
     python -m fwi3d_b200.precond compare --weights W.npz --iterations 5 --out C.json
+    python -m fwi3d_b200.precond time --n 128 --steps 20 --warmup 2
 
 Input normalisation (per volume): the raw gradient below the depth mask,
 divided by its 99.5th percentile of |g| and clipped to [-4, 4]; (v - 2500)/1000;
@@ -127,6 +128,39 @@ def summarise(plain, learned):
     return out
 
 
+def time_network(n=128, steps=20, warmup=2, seed=0):
+    """Device time of the network on an n^3 volume (CUDA events): forward
+    (input packing + 4 layers) and a training step (forward, loss, backward,
+    Adam).  Random inputs; each warm-up step is one forward + one training
+    step at lr 0."""
+    import torch
+    net = lib.Cnn(seed)
+    shape = (n, n, n)
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    x = torch.randn(3, n, n, n, device="cuda", generator=g)
+    y = torch.randn(n, n, n, device="cuda", generator=g) * 0.1
+    out = torch.empty(n, n, n, device="cuda")
+    for _ in range(warmup):
+        net.forward(shape, x.data_ptr(), out.data_ptr())
+        net.train_step(shape, x.data_ptr(), y.data_ptr(), 0.0)
+    torch.cuda.synchronize()
+
+    def timed(f):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            f()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    fwd = timed(lambda: net.forward(shape, x.data_ptr(), out.data_ptr()))
+    trn = timed(lambda: net.train_step(shape, x.data_ptr(), y.data_ptr(), 1e-5))
+    flop = 2 * 27 * (3 * 16 + 16 * 16 + 16 * 16 + 16 * 1) * n ** 3
+    return {"n": n, "steps": steps, "forward_ms": fwd, "train_step_ms": trn,
+            "forward_tflops_algorithmic": flop / (fwd * 1e-3) / 1e12}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -146,6 +180,10 @@ def main(argv=None):
     c.add_argument("--nt", type=int, default=2001)
     c.add_argument("--batch", type=int, default=4)
     c.add_argument("--out", required=True)
+    t = sub.add_parser("time", help="device time of the network's forward and training step")
+    t.add_argument("--n", type=int, default=128)
+    t.add_argument("--steps", type=int, default=20)
+    t.add_argument("--warmup", type=int, default=2)
     a = ap.parse_args(argv)
 
     if a.cmd == "pipeline":
@@ -180,6 +218,8 @@ def main(argv=None):
         print(json.dumps({k: v for k, v in res.items() if k not in ("loss_history", "fwi_holdout")}), flush=True)
         for r in res["fwi_holdout"]:
             print(json.dumps({k: v for k, v in r.items() if k not in ("plain", "learned")}), flush=True)
+    elif a.cmd == "time":
+        print(json.dumps(time_network(a.n, a.steps, a.warmup)), flush=True)
     elif a.cmd == "compare":
         w = getattr(synth, a.workload)(nt=a.nt)
         prob = fwi.Fwi(w, fwi.FwiOptions(batch=a.batch, zmask=w.zmask, rbc=w.rbc))
