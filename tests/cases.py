@@ -9,7 +9,7 @@ from fwi3d_b200 import lib, synth
 
 # Tolerances (relative L2 error of the FP32 CUDA path against the FP64 oracle).
 # The stencil, the wavefields and the accumulators are FP32; the oracle is FP64
-# throughout.  Measured values are recorded in DESIGN.md.
+# throughout.
 TOL_SEIS = 2e-5
 TOL_IMAGE = 2e-4
 TOL_GRAD = 2e-4
