@@ -12,12 +12,14 @@
 //   update_model       m -= step g, v = 1/sqrt(m), model_FWI_iteration_{it}_... file
 // then convergence_{max_iteration}_iterations.txt and final_model_FWI_... .
 //
-// Default behaviour reproduces the reference, quirks included (the device
-// model keeps the 0.05 dm trial model after the line search, the
-// illumination accumulates over every gradient, no d2/dy2 term, no source
-// removal in the rebuild).  b200_fixes = 1 uploads the updated model, zeroes
-// the illumination per gradient, keeps d2/dy2, removes the source and bounds
-// the line-search step to [0, 4 x the largest trial step].
+// By default (b200_fixes = 1) the loop corrects the reference's quirks: it
+// uploads the updated model, zeroes the illumination per gradient, keeps
+// d2/dy2, removes the source in the rebuild and bounds the line-search step to
+// [0, 4 x the largest trial step].  b200_fixes = 0 reproduces the reference
+// for parity, quirks included: the device model keeps the 0.05 dm trial model
+// after the line search, the illumination accumulates over every gradient,
+// there is no d2/dy2 term and no source removal, and the step is unbounded
+// except for the CFL check.
 // The misfit sums are FP64 on the GPU (the reference sums in FP32 on the host).
 #include <fstream>
 
@@ -157,7 +159,7 @@ int main(int argc, char **argv)
         I.res_folder = fwh::param(pf, "inv_residuo_folder");
         I.max_iteration = fwh::param_i(pf, "max_iteration");
         I.seed = fwh::opt_i(pf, "b200_seed", 1);
-        I.fixes = fwh::opt_i(pf, "b200_fixes", 0) != 0;
+        I.fixes = fwh::opt_i(pf, "b200_fixes", 1) != 0;
         const fwh::Model &m = I.m;
         I.npts = (size_t)m.nz * m.nx * m.ny;
         I.per_shot = (size_t)m.nt * m.rec.n;

@@ -7,7 +7,8 @@
 // (export_seismic, migration.cu:137-164).
 // Optional keys: b200_batch (shots per launch), b200_seed (random-boundary
 // seed of shot s is b200_seed + s; the reference seeds from the clock),
-// b200_fixes = 1 (remove the source while rebuilding the forward field).
+// b200_fixes (default 1: remove the source while rebuilding the forward
+// field; 0: keep it, as the reference does).
 #include "workflow.hpp"
 
 int main(int argc, char **argv)
@@ -27,7 +28,7 @@ int main(int argc, char **argv)
         const std::string out_folder = fwh::param(pf, "mig_output_folder");
         const int batch = std::max(1, fwh::opt_i(pf, "b200_batch", 1));
         const int seed = fwh::opt_i(pf, "b200_seed", 1);
-        const int flags = fwh::opt_i(pf, "b200_fixes", 0) ? FWI_FLAG_SUBTRACT_SOURCE : 0;
+        const int flags = fwh::opt_i(pf, "b200_fixes", 1) ? FWI_FLAG_SUBTRACT_SOURCE : 0;
         const int nb = fwh::pad_cells(length, m.dh);
         fwi_ctx *ctx = fwh::make_context(m, nb, FWI_BOUNDARY_RBC, 0.0f, 1, flags);
         fwh::check(fwi_set_velocity(ctx, m.vp.data()), ctx, "fwi_set_velocity");
