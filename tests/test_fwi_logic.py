@@ -49,8 +49,10 @@ def test_step_is_bounded_when_the_parabola_extrapolates():
     p = FakeProblem(vt, v0)
     dm = 1 / 1500.0 ** 2 - 1 / 3000.0 ** 2
     g, _, _, f0 = p.gradient(v0)
-    _, step, _ = p.line_search(v0, g, f0, dm)
+    v1, step, _ = p.line_search(v0, g, f0, dm)
     assert step <= fwi.STEP_BOUND * 0.05 * dm * (1 + 1e-12)
+    # the trust region: no velocity moves by more than MAX_DV
+    assert np.max(np.abs(v1.astype(np.float64) / v0 - 1.0)) <= fwi.MAX_DV * (1 + 1e-5)
 
 
 def test_zero_or_non_finite_gradient_gives_no_step():
