@@ -76,3 +76,30 @@ def test_padding_channels_stay_zero_and_training_lowers_the_loss():
     assert losses[-1] < 0.5 * losses[0], losses[::10]
     w, b = net.get_weights()
     assert np.all(w[0][:, :, 3:] == 0) and np.all(w[3][:, 1:, :] == 0) and np.all(b[3][1:] == 0)
+
+
+def test_training_step_is_reproducible():
+    """Fixed-order partial sums: the same step twice gives the same bits."""
+    net = lib.Cnn(seed=9)
+    inp, target = _inputs(10)
+    x, t = _dev(inp), _dev(target)
+    a = net.train_step(SHAPE, x.data_ptr(), t.data_ptr(), 0.0, want_grads=True)
+    b = net.train_step(SHAPE, x.data_ptr(), t.data_ptr(), 0.0, want_grads=True)
+    assert a[0] == b[0]
+    assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
+
+
+def test_forward_matches_oracle_when_tile_runs_cross_planes():
+    """A volume whose y planes hold many 120-row tile positions, so that the
+    persistent CTAs' tile ranges start and end inside planes."""
+    import torch
+    shape = (40, 36, 30)
+    net = lib.Cnn(seed=11)
+    w, b = _random_weights(net, 12)
+    inp, _ = _inputs(13, shape)
+    x = _dev(inp)
+    out = torch.empty(inp[0].size, device="cuda")
+    net.forward(shape, x.data_ptr(), out.data_ptr())
+    got = out.cpu().numpy().reshape(inp.shape[1:])
+    ref_bf, _ = co.forward(inp, w, b, round_bf16=True)
+    assert rel_l2(got, ref_bf) < 2e-3
