@@ -370,7 +370,8 @@ __global__ void rbc_blobs_kernel(float *__restrict__ vp, int nzz, int nxx, int n
         float v = vp[c];
         for (int q = bin_first[b]; q < bin_first[b + 1]; ++q) {
             const Blob bl = blobs[bin_list[q]];
-            const float ex = (X - bl.x) / bl.r, ey = (Y - bl.y) / bl.r, ez = (Z - bl.z) / bl.r;
+            const float ir = 1.0f / bl.r;
+            const float ex = (X - bl.x) * ir, ey = (Y - bl.y) * ir, ez = (Z - bl.z) * ir;
             const float e2 = ex * ex + ey * ey + ez * ez;
             if (e2 > 25.0f) continue;
             v += bl.amp * expf(-0.5f * e2);

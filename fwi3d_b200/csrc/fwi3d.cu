@@ -485,6 +485,10 @@ void tiling(const fwi_ctx *c, const KInfo &k, int nchunk, int &ntz, int &ntx, in
 void prepare_kernel(const KInfo &k)
 {
     CK(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem));
+    // the whole unified L1 as shared memory: without the preference the driver
+    // may pick a smaller carveout and fit fewer CTAs than the rings allow
+    CK(cudaFuncSetAttribute(k.fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                            (int)cudaSharedmemCarveoutMaxShared));
 }
 
 // Chunks along y so that the grid fills the GPU about twice per resident wave.
