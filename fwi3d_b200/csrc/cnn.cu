@@ -402,43 +402,55 @@ __global__ void __launch_bounds__(tc::THREADS, tc::CTAS_PER_SM)
 // tcgen05 weight gradient.
 //   dW[t][co][ci] = sum_v dy[v][co] x[v + off_t][ci]
 //                 = sum_u dy[u - dz][co] x[u + NZ2 dx + NZ2 NX2 dy][ci]   (u = v + dz)
-// over every padded row (halo rows of dy are zero).  Each CTA owns a range of
-// 128-row blocks of u.  Per block, TMA brings the x rows of the nine (dx, dy)
-// offsets and the dy rows shifted by dz = -1, 0, +1, all as 32-byte-swizzled
-// rows: MN-major operands whose K is the row.
-//   - A, group 1: the x blocks of offsets 0..7 stacked along M (8 x 16 ci).
-//   - A, group 2: the x block of offset 8, then a block of ones in channel 0
-//     (M rows 16..31), then six blocks of group 1 whose rows are not used.
-//     Row 16 against the dz = 0 columns is sum_u dy[u][co]: the bias gradient.
-//   - B: the three dy blocks side by side along N (N = 3 x 16 co).
-// Each 16-row K step is two MMAs (M = 128, N = 48, K = 16) into two
-// accumulators that live in tensor memory for the whole row range.  The
-// epilogue writes per-CTA partials [cta][27][16 co][16 ci] and [cta][16],
-// summed in a fixed order by reduce_partials_kernel.
+// over every padded row (halo rows of dy are zero).  Rows are addressed as
+// (row within a y plane, plane) through 3-D tensor maps of extent (P, ny+2),
+// P = NZ2 NX2, so that a 128-row block never runs into the next plane (rows
+// past P read as zeros) and every u is counted once.
+//
+// Blocks of u stream along y like the convolution's tiles: block (pos, k) is
+// rows pos*128 .. pos*128+127 of plane k, and a CTA owns a contiguous range of
+// blocks in (pos, k) order.  The x rows of block k come from planes k-1, k,
+// k+1 (dy = -1, 0, +1), each plane three blocks at x offsets -1, 0, +1, held
+// in a ring of plane slots: one new plane per block.  Per block, TMA also
+// brings the dy rows shifted by dz = -1, 0, +1.  All operands are 32-byte
+// swizzled rows, MN-major with K = the row.
+//   - A (per plane dy): [x block dx=-1][dx=0][dx=+1][ones in channel 0] and
+//     four more blocks of whatever follows in shared memory, whose rows are not
+//     used: M rows 16 (dx+1) + ci, and row 48 = the ones.
+//   - B: the three dy blocks side by side (N = 3 dz x 16 co).
+// Each 16-row K step is three MMAs (M = 128, N = 48, K = 16), one per plane,
+// into three accumulators that live in tensor memory for the CTA's whole
+// range.  Row 48 of the dy = 0 accumulator against the dz = 0 columns is
+// sum_u dy[u][co], the bias gradient.  The epilogue writes per-CTA partials
+// [cta][27][16 co][16 ci] and [cta][16], summed in a fixed order by
+// reduce_partials_kernel.
 // ---------------------------------------------------------------------------
 namespace wg {
 constexpr int BK = 128;                        // rows of u per block (K)
 constexpr int BLK = BK * CH * 2;               // one block: 128 swizzled 32-byte rows
-// stage: [x block 8][ones][x blocks 0..7][dy blocks dz = -1, 0, +1]
-constexpr int OFF_B8 = 0, OFF_ONES = BLK, OFF_G1 = 2 * BLK, OFF_DY = 10 * BLK;
-constexpr int STAGE = 13 * BLK;
-constexpr int NSTAGE = 2;
+constexpr int PSLOT = 4 * BLK;                 // plane slot: x blocks dx = -1, 0, +1 and the ones block
+constexpr int PS = 4;                          // plane slots (a block reads 3)
+constexpr int TAIL = 4 * BLK;                  // read, never used, by the last slot's MMA (M spans 8 blocks)
+constexpr int DSTAGE = 3 * BLK;                // dy blocks dz = -1, 0, +1
+constexpr int ND = 2;                          // dy stages
+constexpr int OFF_DY = PS * PSLOT + TAIL;
 constexpr int THREADS = 192;
 constexpr int CTAS_PER_SM = 2;
 constexpr int NG = 3 * CH;                     // MMA N: (z tap, c_out)
-constexpr uint32_t TMEM_COLS = 128;            // two 48-column accumulators
-constexpr uint32_t LOAD_BYTES = 12 * BLK;
-constexpr int BAR_BYTES = (2 * NSTAGE + 1) * 8;
-constexpr int SMEM = NSTAGE * STAGE + BAR_BYTES + 16;
+constexpr uint32_t TMEM_COLS = 256;            // three 48-column accumulators
+constexpr int BAR_BYTES = (2 * PS + 2 * ND + 1) * 8;
+constexpr int SMEM = OFF_DY + ND * DSTAGE + BAR_BYTES + 16;
 constexpr uint32_t IDESC = fwi::umma_idesc_bf16(128, NG, true, true);
-static_assert(STAGE % 1024 == 0, "stage alignment");
-static_assert(2 * NG <= (int)TMEM_COLS, "accumulator columns");
+static_assert(PSLOT % 1024 == 0 && DSTAGE % 1024 == 0, "swizzle atom alignment");
+static_assert(3 * NG <= (int)TMEM_COLS, "accumulator columns");
+static_assert(PS >= 4 && PS < 32 && ND < 32, "slot bitmasks");
 }  // namespace wg
 
 struct WgradArgs {
     Geo g;
-    int nkb;           // 128-row blocks of u
-    int kb_per_cta;
+    int ny2;           // y planes
+    int ntiles;        // blocks of u: ceil(P / 128) positions x ny2 planes
+    int tiles_per_cta;
     float *partial;    // [gridDim.x][27][16][16]
     float *bpartial;   // [gridDim.x][16]
 };
@@ -449,9 +461,13 @@ __global__ void __launch_bounds__(wg::THREADS, wg::CTAS_PER_SM)
 {
     using namespace wg;
     extern __shared__ __align__(1024) unsigned char smem[];
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem + NSTAGE * STAGE);
-    uint64_t *empty = full + NSTAGE;
-    uint64_t *done = empty + NSTAGE;
+    unsigned char *ring = smem;
+    unsigned char *dyb = smem + OFF_DY;
+    uint64_t *pfull = reinterpret_cast<uint64_t *>(smem + OFF_DY + ND * DSTAGE);
+    uint64_t *pempty = pfull + PS;
+    uint64_t *dfull = pempty + PS;
+    uint64_t *dempty = dfull + ND;
+    uint64_t *done = dempty + ND;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
@@ -461,21 +477,25 @@ __global__ void __launch_bounds__(wg::THREADS, wg::CTAS_PER_SM)
         return;
     }
     if (threadIdx.x == 0) {
-        for (int s = 0; s < NSTAGE; ++s) {
-            mbar_init(&full[s], 1);
-            mbar_init(&empty[s], 1);
+        for (int s = 0; s < PS; ++s) {
+            mbar_init(&pfull[s], 1);
+            mbar_init(&pempty[s], 1);
+        }
+        for (int s = 0; s < ND; ++s) {
+            mbar_init(&dfull[s], 1);
+            mbar_init(&dempty[s], 1);
         }
         mbar_init(done, 1);
         *abort_flag = 0;
         fwi::fence_mbar_init();
     }
-    // the ones block of every stage: channel 0 = 1 in every row.  In the
+    // the ones block of every plane slot: channel 0 = 1 in every row.  In the
     // 32-byte swizzle, the 16-byte half h of row r sits at half h ^ (r/4 % 2).
-    for (int i = threadIdx.x; i < NSTAGE * BK * 2; i += blockDim.x) {
-        const int st = i / (BK * 2), r = (i >> 1) % BK, h = i & 1;
+    for (int i = threadIdx.x; i < PS * BK * 2; i += blockDim.x) {
+        const int sl = i / (BK * 2), r = (i >> 1) % BK, h = i & 1;
         const int logical = h ^ ((r >> 2) & 1);
         const uint4 v = make_uint4(logical == 0 ? 0x3F80u : 0u, 0u, 0u, 0u);  // BF16 1.0 in channel 0
-        *reinterpret_cast<uint4 *>(smem + st * STAGE + OFF_ONES + r * 32 + h * 16) = v;
+        *reinterpret_cast<uint4 *>(ring + sl * PSLOT + 3 * BLK + r * 32 + h * 16) = v;
     }
     fwi::fence_proxy_async();
     if (warp == 1) fwi::tmem_alloc(tmem_slot, TMEM_COLS);
@@ -483,73 +503,108 @@ __global__ void __launch_bounds__(wg::THREADS, wg::CTAS_PER_SM)
     __syncthreads();
     fwi::tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    const long long kb0 = (long long)blockIdx.x * a.kb_per_cta;
-    const long long kb1 = kb0 + a.kb_per_cta < a.nkb ? kb0 + a.kb_per_cta : a.nkb;
-    const long long plane_xy = (long long)a.g.NZ2 * a.g.NX2;
+    const int T0 = blockIdx.x * a.tiles_per_cta;
+    const int T1 = min(T0 + a.tiles_per_cta, a.ntiles);
 
     if (warp == 0) {
         if (lane == 0) {
             fwi::prefetch_tmap(&mx);
             fwi::prefetch_tmap(&mdy);
-            uint32_t used = 0, phases = 0;
-            int st = 0;
-            uint32_t ph = 0;
-            for (long long kb = kb0; kb < kb1 && !*abort_flag; ++kb) {
-                if (!mbar_wait(&empty[st], ph ^ 1u)) {
-                    cnn_fail(abort_flag);
-                    break;
-                }
-                unsigned char *base = smem + st * STAGE;
-                mbar_expect_tx(&full[st], LOAD_BYTES);
-                const long long u0 = kb * BK;
-                for (int j = 0; j < 9; ++j) {
-                    const int dx = j % 3 - 1, dy = j / 3 - 1;
-                    const long long r = u0 + dx * (long long)a.g.NZ2 + dy * plane_xy;
-                    fwi::tma_load_2d(base + (j < 8 ? OFF_G1 + j * BLK : OFF_B8), &mx, &full[st], 0, (int)r);
-                }
-                for (int k = 0; k < 3; ++k)  // dy rows u - dz, dz = k - 1
-                    fwi::tma_load_2d(base + OFF_DY + k * BLK, &mdy, &full[st], 0, (int)(u0 - (k - 1)));
-                used |= 1u << st;
-                phases = (phases & ~(1u << st)) | (ph << st);
-                if (++st == NSTAGE) {
-                    st = 0;
-                    ph ^= 1u;
-                }
+            uint32_t pused = 0, pph = 0, dused = 0, dph = 0;
+            unsigned g = 0, d = 0;  // planes and dy stages issued
+            bool stop = false;
+            auto issue_plane = [&](int pos, int kp) {
+                const int slot = (int)(g % PS);
+                const uint32_t ph = (g / PS) & 1u;
+                if (*abort_flag || !mbar_wait(&pempty[slot], ph ^ 1u)) return false;
+                mbar_expect_tx(&pfull[slot], 3 * BLK);
+#pragma unroll
+                for (int bx = 0; bx < 3; ++bx)
+                    fwi::tma_load_3d(ring + slot * PSLOT + bx * BLK, &mx, &pfull[slot], 0,
+                                     pos * BK + (bx - 1) * a.g.NZ2, kp);
+                pused |= 1u << slot;
+                pph = (pph & ~(1u << slot)) | (ph << slot);
+                ++g;
+                return true;
+            };
+            auto issue_dy = [&](int pos, int k) {
+                const int st = (int)(d % ND);
+                const uint32_t ph = (d / ND) & 1u;
+                if (*abort_flag || !mbar_wait(&dempty[st], ph ^ 1u)) return false;
+                mbar_expect_tx(&dfull[st], DSTAGE);
+#pragma unroll
+                for (int kk = 0; kk < 3; ++kk)  // dy rows u - dz, dz = kk - 1
+                    fwi::tma_load_3d(dyb + st * DSTAGE + kk * BLK, &mdy, &dfull[st], 0, pos * BK - (kk - 1), k);
+                dused |= 1u << st;
+                dph = (dph & ~(1u << st)) | (ph << st);
+                ++d;
+                return true;
+            };
+            for (int T = T0; T < T1 && !stop;) {
+                const int pos = T / a.ny2, ks = T % a.ny2;
+                const int te = min(T1, (pos + 1) * a.ny2);
+                stop = !issue_plane(pos, ks - 1) || !issue_plane(pos, ks);
+                for (int i = 0; i < te - T && !stop; ++i)
+                    stop = !issue_plane(pos, ks + i + 1) || !issue_dy(pos, ks + i);
+                T = te;
             }
-            for (int s = 0; s < NSTAGE; ++s)
-                if ((used >> s) & 1u)
-                    if (!mbar_wait(&full[s], (phases >> s) & 1u)) atomicOr(&g_cnn_status, 1u);
+            if (stop) cnn_fail(abort_flag);
+            // no copy may land after the CTA has gone
+            for (int s = 0; s < PS; ++s)
+                if ((pused >> s) & 1u)
+                    if (!mbar_wait(&pfull[s], (pph >> s) & 1u)) atomicOr(&g_cnn_status, 1u);
+            for (int s = 0; s < ND; ++s)
+                if ((dused >> s) & 1u)
+                    if (!mbar_wait(&dfull[s], (dph >> s) & 1u)) atomicOr(&g_cnn_status, 1u);
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            const uint32_t s_a = smem_addr(smem);
-            int st = 0;
-            uint32_t ph = 0;
-            bool first = true;
-            for (long long kb = kb0; kb < kb1 && !*abort_flag; ++kb) {
-                if (!mbar_wait(&full[st], ph)) {
-                    cnn_fail(abort_flag);
-                    break;
-                }
-                fwi::tc_fence_after();
-                const uint32_t base = s_a + st * STAGE;
+            const uint32_t ring_a = smem_addr(ring), dy_a = smem_addr(dyb);
+            unsigned g = 0, d = 0;
+            bool first = true, stop = false;
+            for (int T = T0; T < T1 && !stop;) {
+                const int pos = T / a.ny2;
+                const int te = min(T1, (pos + 1) * a.ny2);
+                const int n = te - T;
+                for (int i = 0; i < n; ++i, ++d) {
+                    // planes i, i+1, i+2 of the run (i, i+1 already waited unless i == 0)
+                    bool ok = !*abort_flag;
+                    for (int jp = (i == 0 ? 0 : 2); ok && jp <= 2; ++jp) {
+                        const unsigned pl = g + i + jp;
+                        ok = mbar_wait(&pfull[pl % PS], (pl / PS) & 1u);
+                    }
+                    const int st = (int)(d % ND);
+                    ok = ok && mbar_wait(&dfull[st], (d / ND) & 1u);
+                    if (!ok) {
+                        cnn_fail(abort_flag);
+                        stop = true;
+                        break;
+                    }
+                    fwi::tc_fence_after();
 #pragma unroll 1
-                for (int s = 0; s < BK / 16; ++s) {
-                    const uint32_t koff = s * 512;  // 16 rows of 32 bytes
-                    const uint64_t bd = fwi::umma_desc(base + OFF_DY + koff, BLK, 256, fwi::kSwizzle32B);
+                    for (int s = 0; s < BK / 16; ++s) {
+                        const uint32_t koff = s * 512;  // 16 rows of 32 bytes
+                        const uint64_t bd =
+                            fwi::umma_desc(dy_a + st * DSTAGE + koff, BLK, 256, fwi::kSwizzle32B);
 #pragma unroll
-                    for (int g = 0; g < 2; ++g) {
-                        const uint64_t ad =
-                            fwi::umma_desc(base + (g ? OFF_B8 : OFF_G1) + koff, BLK, 256, fwi::kSwizzle32B);
-                        fwi::umma_bf16(tmem + (uint32_t)(g * NG), ad, bd, IDESC, (first && s == 0) ? 0u : 1u);
+                        for (int p = 0; p < 3; ++p) {  // plane k - 1 + p, i.e. dy = p - 1
+                            const unsigned pl = g + i + p;
+                            const uint64_t ad =
+                                fwi::umma_desc(ring_a + (pl % PS) * PSLOT + koff, BLK, 256, fwi::kSwizzle32B);
+                            fwi::umma_bf16(tmem + (uint32_t)(p * NG), ad, bd, IDESC, (first && s == 0) ? 0u : 1u);
+                        }
+                    }
+                    first = false;
+                    fwi::umma_commit(&dempty[st]);
+                    // plane i is not read again; at the end of the run neither are i+1, i+2
+                    fwi::umma_commit(&pempty[(g + i) % PS]);
+                    if (i == n - 1) {
+                        fwi::umma_commit(&pempty[(g + i + 1) % PS]);
+                        fwi::umma_commit(&pempty[(g + i + 2) % PS]);
                     }
                 }
-                first = false;
-                fwi::umma_commit(&empty[st]);
-                if (++st == NSTAGE) {
-                    st = 0;
-                    ph ^= 1u;
-                }
+                g += n + 2;
+                T = te;
             }
             fwi::umma_commit(done);
         }
@@ -559,26 +614,23 @@ __global__ void __launch_bounds__(wg::THREADS, wg::CTAS_PER_SM)
         const bool ok = __all_sync(0xffffffffu, mbar_wait(done, 0));
         if (ok) {
             fwi::tc_fence_after();
-            const bool empty_range = kb0 >= kb1;
-            const int m = 32 * q + lane;  // accumulator row
+            const bool empty_range = T0 >= T1;
+            const int m = 32 * q + lane;  // accumulator row: 16 (dx+1) + ci, or 48 for the ones
             float *P = a.partial + (long long)blockIdx.x * WSZ;
 #pragma unroll 1
-            for (int acc = 0; acc < 6; ++acc) {
-                // accumulator g = acc / 3, columns of z tap dz = acc % 3 - 1
+            for (int acc = 0; acc < 9; ++acc) {
+                // plane p = acc / 3 (dy = p - 1), columns of z tap dz = acc % 3 - 1
                 uint32_t v[16];
                 fwi::tmem_ld16(tmem + (uint32_t)acc * CH + ((uint32_t)(32 * q) << 16), v);
                 fwi::tmem_wait_ld();
-                const int g = acc / 3, dz = acc % 3 - 1;
-                int j = -1, ci = m % CH;
-                if (g == 0) j = m / CH;
-                else if (m < CH) j = 8;
-                if (j >= 0) {
-                    const int t = (dz + 1) + 3 * (j % 3) + 9 * (j / 3);
+                const int p = acc / 3, dz = acc % 3 - 1;
+                if (m < NG) {
+                    const int dx = m / CH - 1, ci = m % CH;
+                    const int t = (dz + 1) + 3 * (dx + 1) + 9 * p;
 #pragma unroll
                     for (int co = 0; co < CH; ++co)
                         P[(t * CH + co) * CH + ci] = empty_range ? 0.0f : __uint_as_float(v[co]);
-                }
-                if (g == 1 && dz == 0 && m == CH) {
+                } else if (m == NG && p == 1 && dz == 0) {
 #pragma unroll
                     for (int co = 0; co < CH; ++co)
                         a.bpartial[(long long)blockIdx.x * CH + co] = empty_range ? 0.0f : __uint_as_float(v[co]);
@@ -762,24 +814,61 @@ namespace {
 // Rows map over a padded BF16 activation buffer: (16 channels, row), box of
 // `box_rows` whole 32-byte rows, 32-byte swizzle (the SW32 operand layout of
 // the tensor-core descriptors).  Rows outside [0, R) read as zeros.
-int rows_map(fwi_cnn *n, const __nv_bfloat16 *base, int box_rows, CUtensorMap *m)
+// The driver's tensor-map encoder, looked up once.
+PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder()
 {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     if (!fn) {
         void *p = nullptr;
         cudaDriverEntryPointQueryResult q;
-        CNN_CK(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q));
-        if (q != cudaDriverEntryPointSuccess || !p) {
-            n->err = "cuTensorMapEncodeTiled unavailable";
-            return FWI_ERR_CUDA;
-        }
-        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess && p)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+int rows_map(fwi_cnn *n, const __nv_bfloat16 *base, int box_rows, CUtensorMap *m)
+{
+    const PFN_cuTensorMapEncodeTiled_v12000 fn = tmap_encoder();
+    if (!fn) {
+        n->err = "cuTensorMapEncodeTiled unavailable";
+        return FWI_ERR_CUDA;
     }
     cuuint64_t dims[2] = {CH, (cuuint64_t)n->g.R};
     cuuint64_t strides[1] = {CH * 2};
     cuuint32_t box[2] = {CH, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
     const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void *)base, dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        n->err = "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")";
+        return FWI_ERR_CUDA;
+    }
+    return FWI_OK;
+}
+
+// Plane map over a padded BF16 activation buffer: (16 channels, row within a
+// y plane, plane) with extents (16, NZ2 NX2, ny + 2), box (16, 128, 1),
+// 32-byte swizzle.  Rows past the end of a plane, and planes outside the
+// volume, read as zeros.
+int plane_map(fwi_cnn *n, const __nv_bfloat16 *base, CUtensorMap *m)
+{
+    const PFN_cuTensorMapEncodeTiled_v12000 fn = tmap_encoder();
+    if (!fn) {
+        n->err = "cuTensorMapEncodeTiled unavailable";
+        return FWI_ERR_CUDA;
+    }
+    const cuuint64_t P = (cuuint64_t)n->g.NZ2 * n->g.NX2;
+    cuuint64_t dims[3] = {CH, P, (cuuint64_t)(n->g.ny + 2)};
+    cuuint64_t strides[2] = {CH * 2, P * CH * 2};
+    cuuint32_t box[3] = {CH, (cuuint32_t)wg::BK, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, (void *)base, dims, strides, box, estr,
                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
@@ -857,12 +946,14 @@ int launch_wgrad(fwi_cnn *n, const __nv_bfloat16 *x, const __nv_bfloat16 *dy, fl
         ctas = std::min(resident_ctas(n, wg::SMEM, wg::TMEM_COLS, wg::CTAS_PER_SM), kMaxPartials);
     }
     CUtensorMap mx, mdy;
-    int st = rows_map(n, x, wg::BK, &mx);
-    if (st == FWI_OK) st = rows_map(n, dy, wg::BK, &mdy);
+    int st = plane_map(n, x, &mx);
+    if (st == FWI_OK) st = plane_map(n, dy, &mdy);
     if (st != FWI_OK) return st;
-    WgradArgs a{n->g, (int)((n->g.R + wg::BK - 1) / wg::BK), 0, n->partial.p, n->bpartial.p};
-    a.kb_per_cta = (a.nkb + ctas - 1) / ctas;
-    const int grid = (a.nkb + a.kb_per_cta - 1) / a.kb_per_cta;
+    const long long P = (long long)n->g.NZ2 * n->g.NX2;
+    const int ny2 = n->g.ny + 2;
+    WgradArgs a{n->g, ny2, (int)((P + wg::BK - 1) / wg::BK) * ny2, 0, n->partial.p, n->bpartial.p};
+    a.tiles_per_cta = (a.ntiles + ctas - 1) / ctas;
+    const int grid = (a.ntiles + a.tiles_per_cta - 1) / a.tiles_per_cta;
     wgrad_tc_kernel<<<grid, wg::THREADS, wg::SMEM, n->stream>>>(mx, mdy, a);
     CNN_CK(cudaGetLastError());
     reduce_partials_kernel<<<(WSZ + RED_X - 1) / RED_X, RED_X * RED_Y, 0, n->stream>>>(n->partial.p, grid, WSZ, gw);
