@@ -48,6 +48,7 @@ constexpr int TAPS = 27;
 constexpr int WSZ = TAPS * CH * CH;  // weights per layer
 constexpr int CIN[NL] = {3, 16, 16, 16};
 constexpr int kMaxPartials = 1024;  // per-CTA weight-gradient partials held
+constexpr int kMaxDevices = 64;     // devices one process can drive
 constexpr int COUT[NL] = {16, 16, 16, 1};
 
 // Division by a run-time invariant d (1 <= d < 2^31) of dividends n < 2^31,
@@ -897,7 +898,15 @@ template <int SIGN, int MODE>
 int launch_conv(fwi_cnn *n, const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias,
                 const __nv_bfloat16 *mask, __nv_bfloat16 *out, float *out32)
 {
-    static int ctas = 0;  // resident CTAs on the whole GPU
+    // kernel attributes are per device: set them, and size the grid, once per device
+    static int ctas_of[kMaxDevices] = {};
+    int dev = 0;
+    CNN_CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) {
+        n->err = "device ordinal beyond the supported count";
+        return FWI_ERR_ARG;
+    }
+    int &ctas = ctas_of[dev];  // resident CTAs on the whole GPU
     if (!ctas) {
         CNN_CK(cudaFuncSetAttribute(conv_tc_kernel<SIGN, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     tc::SMEM));
@@ -938,7 +947,14 @@ int forward_impl(fwi_cnn *n)
 // rows, dy = the gradient rows of its output.
 int launch_wgrad(fwi_cnn *n, const __nv_bfloat16 *x, const __nv_bfloat16 *dy, float *gw, float *gb)
 {
-    static int ctas = 0;
+    static int ctas_of[kMaxDevices] = {};  // per device, as in launch_conv
+    int dev = 0;
+    CNN_CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) {
+        n->err = "device ordinal beyond the supported count";
+        return FWI_ERR_ARG;
+    }
+    int &ctas = ctas_of[dev];
     if (!ctas) {
         CNN_CK(cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, wg::SMEM));
         CNN_CK(cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
