@@ -294,7 +294,7 @@ def run_ours(args, ws, rank, local):
                 ctx.apply_random_boundary(seed=1000 + s, **rbc)
                 if rtm:
                     ctx.rtm_shots([s], host[s].numpy())
-                    out.numpy()[:] = ctx.rtm_image().ravel()
+                    ctx.rtm_image(out=out.numpy())  # straight into the pinned host buffer
                     h2d += host[s].numel() * 4
                     d2h += out.numel() * 4
                 else:

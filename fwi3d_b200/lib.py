@@ -314,8 +314,14 @@ class Context:
         """Replace the accumulators by caller device buffers (dense padded)."""
         self._check(self.lib.fwi_set_accumulators_dev(self.h, C.c_void_p(d_img or None), C.c_void_p(d_ill or None)))
 
-    def rtm_image(self) -> np.ndarray:
-        out = np.empty(self.model_shape, np.float32)
+    def rtm_image(self, out: np.ndarray | None = None) -> np.ndarray:
+        """The post-processed image (model shape).  `out`, if given, is a
+        C-contiguous float32 host array of the model's size (for example a view
+        of pinned memory) that receives it without an extra copy."""
+        if out is None:
+            out = np.empty(self.model_shape, np.float32)
+        elif out.dtype != np.float32 or not out.flags["C_CONTIGUOUS"] or out.size != int(np.prod(self.model_shape)):
+            raise ValueError("out must be a C-contiguous float32 array of the model's size")
         self._check(self.lib.fwi_rtm_image(self.h, _fptr(out)))
         return out
 
