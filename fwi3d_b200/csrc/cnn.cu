@@ -27,6 +27,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <random>
 #include <string>
 #include <vector>
@@ -898,23 +899,30 @@ template <int SIGN, int MODE>
 int launch_conv(fwi_cnn *n, const __nv_bfloat16 *in, const __nv_bfloat16 *w, const float *bias,
                 const __nv_bfloat16 *mask, __nv_bfloat16 *out, float *out32)
 {
-    // kernel attributes are per device: set them, and size the grid, once per device
+    // kernel attributes are per device: set them, and size the grid, once per
+    // device; host threads that drive the same device take the lock first
     static int ctas_of[kMaxDevices] = {};
+    static std::mutex lock_of[kMaxDevices];
     int dev = 0;
     CNN_CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) {
         n->err = "device ordinal beyond the supported count";
         return FWI_ERR_ARG;
     }
-    int &ctas = ctas_of[dev];  // resident CTAs on the whole GPU
-    if (!ctas) {
+    int ctas = 0;  // resident CTAs on the whole GPU
+    {
+        std::lock_guard<std::mutex> guard(lock_of[dev]);
+        if (!ctas_of[dev]) {
         CNN_CK(cudaFuncSetAttribute(conv_tc_kernel<SIGN, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     tc::SMEM));
         // the whole unified L1 as shared memory, so that four CTAs fit
         CNN_CK(cudaFuncSetAttribute(conv_tc_kernel<SIGN, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                     (int)cudaSharedmemCarveoutMaxShared));
-        ctas = resident_ctas(n, tc::SMEM, tc::TMEM_COLS, tc::CTAS_PER_SM);
-        if (ctas <= 0) return FWI_ERR_CUDA;
+            const int c = resident_ctas(n, tc::SMEM, tc::TMEM_COLS, tc::CTAS_PER_SM);
+            if (c <= 0) return FWI_ERR_CUDA;
+            ctas_of[dev] = c;
+        }
+        ctas = ctas_of[dev];
     }
     CUtensorMap m;
     const int st = rows_map(n, in, tc::SEG, &m);
@@ -947,19 +955,26 @@ int forward_impl(fwi_cnn *n)
 // rows, dy = the gradient rows of its output.
 int launch_wgrad(fwi_cnn *n, const __nv_bfloat16 *x, const __nv_bfloat16 *dy, float *gw, float *gb)
 {
-    static int ctas_of[kMaxDevices] = {};  // per device, as in launch_conv
+    static int ctas_of[kMaxDevices] = {};  // per device, under a lock, as in launch_conv
+    static std::mutex lock_of[kMaxDevices];
     int dev = 0;
     CNN_CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) {
         n->err = "device ordinal beyond the supported count";
         return FWI_ERR_ARG;
     }
-    int &ctas = ctas_of[dev];
-    if (!ctas) {
-        CNN_CK(cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, wg::SMEM));
-        CNN_CK(cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                    (int)cudaSharedmemCarveoutMaxShared));
-        ctas = std::min(resident_ctas(n, wg::SMEM, wg::TMEM_COLS, wg::CTAS_PER_SM), kMaxPartials);
+    int ctas = 0;
+    {
+        std::lock_guard<std::mutex> guard(lock_of[dev]);
+        if (!ctas_of[dev]) {
+            CNN_CK(cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, wg::SMEM));
+            CNN_CK(cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        (int)cudaSharedmemCarveoutMaxShared));
+            const int c = std::min(resident_ctas(n, wg::SMEM, wg::TMEM_COLS, wg::CTAS_PER_SM), kMaxPartials);
+            if (c <= 0) return FWI_ERR_CUDA;
+            ctas_of[dev] = c;
+        }
+        ctas = ctas_of[dev];
     }
     CUtensorMap mx, mdy;
     int st = plane_map(n, x, &mx);

@@ -109,6 +109,9 @@ extern "C" int fwi_residual_noalloc(const float *d_obs, const float *d_cal, int6
                                     double *d_sum_sq, void *stream)
 {
     if (!d_obs || !d_cal || !d_sum_sq || n < 0) return FWI_ERR_ARG;
+    // a non-sticky error left by an earlier call (this library's or another's)
+    // must not be reported as this call's launch failure
+    cudaGetLastError();
     if (n > FWI_NOALLOC_MAX_N) {
         fprintf(stderr,
                 "fwi_residual_noalloc: n = %lld exceeds the no-alloc scratch limit of %lld samples "

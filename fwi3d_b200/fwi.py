@@ -124,12 +124,18 @@ class Fwi:
         """Bounded parabolic step on m = 1/v^2, within the MAX_DV trust
         region.  Returns (new velocity, step, the parabola's predicted misfit
         at the step)."""
-        if not np.all(np.isfinite(g)) or not np.any(g):
+        if not (dm > 0) or not np.all(np.isfinite(g)) or not np.any(g):
             return v, 0.0, f0
         m = 1.0 / (v.astype(np.float64) ** 2)
+        g64 = np.asarray(g, np.float64)
         a = np.array([0.0, 0.02 * dm, 0.05 * dm])
         lo, hi = self.vbounds
-        trial = lambda alpha: np.clip(1.0 / np.sqrt(np.maximum(m - alpha * g, 1e-12)), lo, hi).astype(np.float32)
+
+        def trial(alpha):
+            # FP64 throughout, whatever the type of alpha: a Python float times
+            # an FP32 array would round the product to FP32, so the same step
+            # would give a slightly different model each way it is written
+            return np.clip(1.0 / np.sqrt(np.maximum(m - float(alpha) * g64, 1e-12)), lo, hi).astype(np.float32)
         f = np.array([f0, self.misfit(trial(a[1])), self.misfit(trial(a[2]))])
         # the reference fits the parabola to sqrt(sum res^2) (inversion.cu:390-403)
         r = np.sqrt(f)

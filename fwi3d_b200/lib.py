@@ -320,8 +320,9 @@ class Context:
         of pinned memory) that receives it without an extra copy."""
         if out is None:
             out = np.empty(self.model_shape, np.float32)
-        elif out.dtype != np.float32 or not out.flags["C_CONTIGUOUS"] or out.size != int(np.prod(self.model_shape)):
-            raise ValueError("out must be a C-contiguous float32 array of the model's size")
+        elif (out.dtype != np.float32 or not out.flags["C_CONTIGUOUS"] or not out.flags["WRITEABLE"]
+              or out.size != int(np.prod(self.model_shape))):
+            raise ValueError("out must be a writable, C-contiguous float32 array of the model's size")
         self._check(self.lib.fwi_rtm_image(self.h, _fptr(out)))
         return out
 

@@ -69,3 +69,24 @@ def test_noalloc_residual_rejects_sizes_beyond_its_scratch():
         lib.residual_noalloc(x.data_ptr(), x.data_ptr(), lib.NOALLOC_MAX_N + 1, 0, out.data_ptr())
     assert e.value.code == 1
     assert lib.NOALLOC_MAX_N == 268435456
+
+
+def test_noalloc_residual_ignores_an_error_left_by_an_earlier_call():
+    """A refused allocation leaves a non-sticky error in the CUDA runtime; the
+    next no-alloc call must not report it as its own launch failure."""
+    import torch
+    ctx = _ctx()
+    tiny = np.zeros(4, np.float32)
+    # the library's device buffer for 3 x 2^41 samples cannot be allocated;
+    # the request is refused before the host arrays are read
+    st = ctx.lib.fwi_residual(ctx.h, lib._fptr(tiny), lib._fptr(tiny), 1 << 41, None,
+                              lib.C.byref(lib.C.c_double()))
+    assert st == 3  # FWI_ERR_ALLOC
+    n = 4099
+    obs = torch.ones(n, device="cuda", dtype=torch.float32)
+    cal = torch.zeros(n, device="cuda", dtype=torch.float32)
+    out = torch.zeros(1, device="cuda", dtype=torch.float64)
+    lib.residual_noalloc(obs.data_ptr(), cal.data_ptr(), n, 0, out.data_ptr())
+    torch.cuda.synchronize()
+    assert float(out.item()) == float(n)
+    ctx.close()
