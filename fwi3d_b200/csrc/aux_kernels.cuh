@@ -290,11 +290,14 @@ __device__ __forceinline__ float uniform01(uint64_t seed, uint64_t stream, uint6
     return ((float)(h >> 40) + 0.5f) * (1.0f / 16777216.0f);
 }
 
+// Box-Muller in FP64, rounded once to FP32: the deviate is then the FP32
+// rounding of a value any FP64 restatement computes to within a few FP64
+// ulps, so a host restatement reproduces it bit for bit.
 __device__ __forceinline__ float normal01(uint64_t seed, uint64_t stream, uint64_t ctr)
 {
-    const float u1 = uniform01(seed, stream, 2 * ctr);
-    const float u2 = uniform01(seed, stream, 2 * ctr + 1);
-    return sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
+    const double u1 = (double)uniform01(seed, stream, 2 * ctr);
+    const double u2 = (double)uniform01(seed, stream, 2 * ctr + 1);
+    return (float)(sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2));
 }
 
 // Pad background.  For every pad cell take the nearest model-edge value, then
@@ -323,16 +326,19 @@ __global__ void rbc_background_kernel(float *__restrict__ vp, int nzz, int nxx, 
         const int dz = pad_depth(i, nzz, nb), dx = pad_depth(j, nxx, nb), dy = pad_depth(k, nyy, nb);
         const uint64_t cell = (uint64_t)i + (uint64_t)nzz * ((uint64_t)j + (uint64_t)nxx * k);
         const float fnb = (float)nb;
+        // every product and sum rounded on its own (no contraction), so that
+        // FP32 arithmetic on the host reproduces the pad exactly
         if (kind == 0) {
-            if (dx >= 0) v += (1.0f - dx / fnb) * varVp * normal01(seed, 1, cell);
-            if (dy >= 0) v += (1.0f - dy / fnb) * varVp * normal01(seed, 2, cell);
-            if (dz >= 0) v += (1.0f - dz / fnb) * varVp * normal01(seed, 3, cell);
+            if (dx >= 0) v = __fadd_rn(v, __fmul_rn(__fmul_rn(1.0f - dx / fnb, varVp), normal01(seed, 1, cell)));
+            if (dy >= 0) v = __fadd_rn(v, __fmul_rn(__fmul_rn(1.0f - dy / fnb, varVp), normal01(seed, 2, cell)));
+            if (dz >= 0) v = __fadd_rn(v, __fmul_rn(__fmul_rn(1.0f - dz / fnb, varVp), normal01(seed, 3, cell)));
         } else {
             float ramp = 0.0f;
             if (dx >= 0) ramp = fmaxf(ramp, 1.0f - dx / fnb);
             if (dy >= 0) ramp = fmaxf(ramp, 1.0f - dy / fnb);
             if (dz >= 0) ramp = fmaxf(ramp, 1.0f - dz / fnb);
-            v *= 1.0f + ratio * ramp * (2.0f * uniform01(seed, 4, cell) - 1.0f);
+            const float u = __fsub_rn(__fmul_rn(2.0f, uniform01(seed, 4, cell)), 1.0f);
+            v = __fmul_rn(v, __fadd_rn(1.0f, __fmul_rn(__fmul_rn(ratio, ramp), u)));
         }
         vp[c] = fminf(fmaxf(v, vlo), vhi);
     }

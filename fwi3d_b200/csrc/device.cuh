@@ -43,6 +43,7 @@ struct FwdArgs {
     float cvel;                   // dt^2 / dh^2
     float idh3;                   // source / adjoint scaling 1/dh^3
     int nb;                       // pad width (damper tables)
+    int vel_slots;                // 1: every shot reads velocity slot 0; B: shot s reads slot s
     float *Q;                     // field written this step (batch base)
     const float *A;               // field read with the stencil (batch base)
     const float *b1d;             // Cerjan 1-D table (ABC only)
@@ -63,6 +64,7 @@ struct BwdArgs {
     float gscale;                 // dt / dh^2 (gradient imaging condition)
     float idh3;
     int subtract_src;             // remove the source while rebuilding Ps
+    int vel_slots;                // 1: every shot reads velocity slot 0; B: shot s reads slot s
     float *Ps;                    // rebuilt source field (written)
     const float *Psold;           // source field read with the stencil
     float *Prold;                 // adjoint field written

@@ -51,10 +51,10 @@ KInfo fwd_info(bool abc)
 {
     using T = TileOf<I>;
     KInfo k;
-    k.threads = T::NT;
+    k.threads = T::THREADS;
     k.tz = T::TZ;
     k.tx = T::TX;
-    k.smem = SHF * T::HSLOT + SCF * 2 * T::CSLOT + (SHF + SCF) * 8;
+    k.smem = SHF * T::HSLOT + SCF * 2 * T::CSLOT + 2 * (SHF + SCF) * 8;  // rings + full/empty barriers
     k.fn = abc ? (const void *)fd_forward_kernel<T, SHF, SCF, true>
                : (const void *)fd_forward_kernel<T, SHF, SCF, false>;
     return k;
@@ -65,10 +65,10 @@ KInfo bwd_info(bool grad, bool dy)
 {
     using T = TileOf<I>;
     KInfo k;
-    k.threads = T::NT;
+    k.threads = T::THREADS;
     k.tz = T::TZ;
     k.tx = T::TX;
-    k.smem = SHB * 2 * T::HSLOT + SCB * 5 * T::CSLOT + (SHB + SCB) * 8;
+    k.smem = SHB * 2 * T::HSLOT + SCB * 5 * T::CSLOT + 2 * (SHB + SCB) * 8;
     if (!grad)
         k.fn = (const void *)fd_backward_kernel<T, SHB, SCB, false, false>;
     else if (dy)
@@ -194,10 +194,11 @@ double stability_velocity(double dh, double dt)
 }
 
 struct GraphKey {
-    int kind, n, tile, nchunk, flags;
+    int kind, n, tile, nchunk, flags, vslots;
     bool operator<(const GraphKey &o) const
     {
-        return std::tie(kind, n, tile, nchunk, flags) < std::tie(o.kind, o.n, o.tile, o.nchunk, o.flags);
+        return std::tie(kind, n, tile, nchunk, flags, vslots) <
+               std::tie(o.kind, o.n, o.tile, o.nchunk, o.flags, o.vslots);
     }
 };
 
@@ -210,10 +211,9 @@ struct Graph {
 struct BlobKey {
     uint64_t seed = 0;
     float xm = 0, ym = 0, zm = 0, ratio = 0, varVp = 0, fnb = 0;
-    bool operator==(const BlobKey &o) const
+    bool operator<(const BlobKey &o) const
     {
-        return seed == o.seed && xm == o.xm && ym == o.ym && zm == o.zm && ratio == o.ratio && varVp == o.varVp &&
-               fnb == o.fnb;
+        return std::tie(seed, xm, ym, zm, ratio, varVp, fnb) < std::tie(o.seed, o.xm, o.ym, o.zm, o.ratio, o.varVp, o.fnb);
     }
 };
 
@@ -222,6 +222,46 @@ struct BlobSet {
     std::vector<int> first, list;
     int nbz = 0, nbx = 0, nby = 0;
     float bin = 0;
+};
+
+BlobSet make_blobs(BlobKey k);
+
+// Blob sets built on host threads ahead of their use: the Poisson-disk
+// sampling takes tens of milliseconds per pad, which overlaps the GPU's work
+// on the previous shot or batch.  Keyed by the recipe and the seed.
+struct BlobCache {
+    std::map<BlobKey, std::shared_future<BlobSet>> pending;
+    void prefetch(const BlobKey &k)
+    {
+        if (pending.count(k)) return;
+        if (pending.size() >= 4 * (size_t)kMaxBatch) drain();  // stale guesses
+        pending.emplace(k, std::async(std::launch::async, make_blobs, k).share());
+    }
+    BlobSet take(const BlobKey &k)
+    {
+        prefetch(k);
+        auto it = pending.find(k);
+        BlobSet b = it->second.get();
+        pending.erase(it);
+        return b;
+    }
+    void drain()
+    {
+        for (auto &kv : pending) kv.second.wait();
+        pending.clear();
+    }
+};
+
+// Device copy of one velocity slot's blob set.
+struct SlotBlobs {
+    DevBuf<Blob> blobs;
+    DevBuf<int> first, list;
+    void release()
+    {
+        blobs.release();
+        first.release();
+        list.release();
+    }
 };
 
 }  // namespace
@@ -261,11 +301,15 @@ struct fwi_ctx {
     DevBuf<unsigned int> ubits;
     DevBuf<float> post;  // [nz*nx*ny] post-processing output
     DevBuf<float> stage;  // host-model uploads and padded downloads
-    DevBuf<Blob> blob_dev;
-    DevBuf<int> bin_first, bin_list;
-    BlobSet blobs_now;               // host copy behind the last blob upload
-    std::future<BlobSet> blobs_next; // blob set of the next seed, built on a host thread
-    BlobKey blobs_next_key;
+    BlobCache blob_cache;
+    SlotBlobs slot_dev[kMaxBatch];   // blob sets of the velocity slots on the device
+    BlobSet slot_host[kMaxBatch];    // their host copies, alive until the uploads ran
+    // velocity slots: vp holds vel_slots padded models; with a random pad per
+    // shot (fwi_set_shot_random_boundary) and B > 1, batch slot s reads slot s
+    int vel_slots = 1;
+    bool shot_rbc = false;
+    fwi_rbc shot_rbc_params{};
+    uint64_t shot_rbc_seed = 0;
     int generation = 0;  // bumped whenever a buffer a graph points at moves
     bool acc_dirty = false;
 
@@ -554,7 +598,7 @@ FwdLaunch make_fwd(fwi_ctx *c, int n, int tile, int nchunk, bool record)
         L.mh[b] = make_map(c->F[b].p, c->nzz, c->nxx, c->nyy, c->ldz, n, L.k.tz + 8, L.k.tx + 8);
         L.mq[b] = make_map(c->F[b].p, c->nzz, c->nxx, c->nyy, c->ldz, n, L.k.tz, L.k.tx);
     }
-    L.mv = make_map(c->vp.p, c->nzz, c->nxx, c->nyy, c->ldz, 1, L.k.tz, L.k.tx);
+    L.mv = make_map(c->vp.p, c->nzz, c->nxx, c->nyy, c->ldz, c->vel_slots, L.k.tz, L.k.tx);
     FwdArgs &a = L.a;
     memset(&a, 0, sizeof a);
     a.nzz = c->nzz;
@@ -570,6 +614,7 @@ FwdLaunch make_fwd(fwi_ctx *c, int n, int tile, int nchunk, bool record)
     a.cvel = c->p.dt * c->p.dt * c->idh2;
     a.idh3 = c->idh3;
     a.nb = c->g.nb;
+    a.vel_slots = c->vel_slots;
     a.b1d = abc ? c->b1d.p : nullptr;
     a.wavelet = c->wavelet.p;
     a.binfo = c->binfo.p;
@@ -610,7 +655,7 @@ BwdLaunch make_bwd(fwi_ctx *c, int n, int tile, int nchunk, bool grad)
         L.mcs[b] = make_map(c->F[b].p, c->nzz, c->nxx, c->nyy, c->ldz, n, L.k.tz, L.k.tx);
         L.mcr[b] = make_map(c->Rf[b].p, c->nzz, c->nxx, c->nyy, c->ldz, n, L.k.tz, L.k.tx);
     }
-    L.mv = make_map(c->vp.p, c->nzz, c->nxx, c->nyy, c->ldz, 1, L.k.tz, L.k.tx);
+    L.mv = make_map(c->vp.p, c->nzz, c->nxx, c->nyy, c->ldz, c->vel_slots, L.k.tz, L.k.tx);
     L.mim = make_map(c->acc_img.p, c->nzz, c->nxx, c->nyy, c->ldz, n, L.k.tz, L.k.tx);
     L.mil = make_map(c->acc_ill.p, c->nzz, c->nxx, c->nyy, c->ldz, n, L.k.tz, L.k.tx);
     BwdArgs &a = L.a;
@@ -629,6 +674,7 @@ BwdLaunch make_bwd(fwi_ctx *c, int n, int tile, int nchunk, bool grad)
     a.gscale = c->p.dt * c->idh2;
     a.idh3 = c->idh3;
     a.subtract_src = (c->p.flags & FWI_FLAG_SUBTRACT_SOURCE) ? 1 : 0;
+    a.vel_slots = c->vel_slots;
     a.image = c->acc_img.p;
     a.illum = c->acc_ill.p;
     a.wavelet = c->wavelet.p;
@@ -673,7 +719,7 @@ Graph &time_loop_graph(fwi_ctx *c, int kind, int n)
     if (nchunk <= 0)
         nchunk = kind < 2 ? default_chunks(c, fwd_kernel(tile, c->p.boundary == FWI_BOUNDARY_ABC), n)
                           : default_chunks(c, bwd_kernel(tile, kind == 3, false), n);
-    GraphKey key{kind, n, tile, nchunk, c->p.flags};
+    GraphKey key{kind, n, tile, nchunk, c->p.flags, c->vel_slots};
     Graph &gr = c->graphs[key];
     if (gr.exec && gr.generation == c->generation) return gr;
     if (gr.exec) {
@@ -772,6 +818,8 @@ void data_from_fortran(fwi_ctx *c, int R, const float *src)
     ++c->launches;
 }
 
+void shot_pads(fwi_ctx *c, const int *ids, int n, const int *next, int n_next);
+
 // Forward modeling of a list of shots in batches of B.
 void model_impl(fwi_ctx *c, const int *shots, int nshots, float *out, bool out_is_device)
 {
@@ -783,6 +831,8 @@ void model_impl(fwi_ctx *c, const int *shots, int nshots, float *out, bool out_i
         const int n = std::min(c->B, nshots - s0);
         BatchTables t = build_batch(c, shots + s0, n);
         upload_batch(c, t);
+        if (c->shot_rbc)
+            shot_pads(c, shots + s0, n, shots + s0 + n, std::min(c->B, nshots - s0 - n));
         const int R = t.info.R;
         if (R) CK(cudaMemsetAsync(c->seis_tm.p, 0, (size_t)c->p.nt * R * sizeof(float), c->stream));
         start_forward(c, n);
@@ -821,6 +871,8 @@ void migrate_impl(fwi_ctx *c, const int *shots, int nshots, const float *data, b
         const int n = std::min(c->B, nshots - s0);
         BatchTables t = build_batch(c, shots + s0, n);
         upload_batch(c, t);
+        if (c->shot_rbc)
+            shot_pads(c, shots + s0, n, shots + s0 + n, std::min(c->B, nshots - s0 - n));
         const int R = t.info.R;
         const size_t cnt = (size_t)c->p.nt * R;
         if (R) {
@@ -1020,11 +1072,11 @@ BlobSet make_blobs(BlobKey k)
     return out;
 }
 
-float device_max_abs(fwi_ctx *c, const float *v)
+float device_max_abs(fwi_ctx *c, const float *v, long long n)
 {
     c->ubits.ensure(1);
     CK(cudaMemsetAsync(c->ubits.p, 0, sizeof(unsigned), c->stream));
-    max_abs_kernel<<<grid_blocks(c->vol), 256, 0, c->stream>>>(v, c->vol, c->ldz, c->nzz, c->ubits.p);
+    max_abs_kernel<<<grid_blocks(n), 256, 0, c->stream>>>(v, n, c->ldz, c->nzz, c->ubits.p);
     CK(cudaGetLastError());
     unsigned bits = 0;
     CK(cudaMemcpyAsync(&bits, c->ubits.p, sizeof bits, cudaMemcpyDeviceToHost, c->stream));
@@ -1034,13 +1086,118 @@ float device_max_abs(fwi_ctx *c, const float *v)
     return f;
 }
 
-void check_cfl(fwi_ctx *c)
+void check_cfl(fwi_ctx *c, int nslots = 1)
 {
-    const float vm = device_max_abs(c, c->vp.p);
+    const float vm = device_max_abs(c, c->vp.p, (long long)nslots * c->vol);
     const double lim = stability_velocity(c->g.dh, c->p.dt);
     if (!(vm <= lim))
         fail(FWI_ERR_NUMERIC, "velocity %.1f m/s exceeds the leapfrog stability limit %.1f m/s (dh=%g, dt=%g)",
              vm, lim, c->g.dh, c->p.dt);
+}
+
+void check_rbc(const fwi_rbc *rbc)
+{
+    if (rbc->kind != 0 && rbc->kind != 1) fail(FWI_ERR_ARG, "unknown random boundary kind %d", rbc->kind);
+    if (!(rbc->ratio >= 0) || !(rbc->varVp >= 0)) fail(FWI_ERR_ARG, "random boundary ratio and varVp must be >= 0");
+}
+
+bool wants_blobs(const fwi_rbc *rbc) { return rbc->kind == 0 && rbc->ratio > 0 && rbc->varVp > 0; }
+
+// Clamp of the pad: kind 0 keeps [vmin - varVp, vmax + varVp] like the
+// reference's blob kernel (src/modeling/modeling.cu:611-612); both kinds stay
+// at or below cfl_cap times the leapfrog stability velocity.
+void rbc_bounds(const fwi_ctx *c, const fwi_rbc *rbc, float &vlo, float &vhi)
+{
+    const double cap = (rbc->cfl_cap > 0 ? rbc->cfl_cap : 0.98) * stability_velocity(c->g.dh, c->p.dt);
+    if (rbc->kind == 0) {
+        vlo = c->vmin - rbc->varVp;
+        vhi = (float)std::min<double>(c->vmax + rbc->varVp, cap);
+        vlo = std::max(vlo, 0.05f * c->vmin);
+    } else {
+        vlo = 0.05f * c->vmin;
+        vhi = (float)cap;
+    }
+}
+
+BlobKey blob_key(const fwi_ctx *c, const fwi_rbc *rbc, uint64_t seed)
+{
+    const float dh = c->g.dh;
+    BlobKey key;
+    key.seed = seed;
+    key.xm = (c->nxx - 1) * dh;
+    key.ym = (c->nyy - 1) * dh;
+    key.zm = (c->nzz - 1) * dh;
+    key.ratio = rbc->ratio;
+    key.varVp = rbc->varVp;
+    key.fnb = c->g.nb * dh;
+    return key;
+}
+
+// Random pad of one seed into velocity slot `slot`, rebuilt from the clean
+// edge-padded model (no drift from one shot to the next).  The host copy of
+// the slot's blob set stays in slot_host until the next pad of that slot, so
+// the asynchronous uploads read valid memory as long as the caller
+// synchronises the stream before reusing the slot.
+void pad_slot(fwi_ctx *c, const fwi_rbc *rbc, uint64_t seed, int slot)
+{
+    float vlo, vhi;
+    rbc_bounds(c, rbc, vlo, vhi);
+    float *dst = c->vp.p + (size_t)slot * c->vol;
+    CK(cudaMemcpyAsync(dst, c->vp_clean.p, c->vol * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
+    rbc_background_kernel<<<grid_blocks(c->vol), 256, 0, c->stream>>>(
+        dst, c->nzz, c->nxx, c->nyy, c->ldz, c->g.nb, rbc->kind, rbc->ratio, rbc->varVp, vlo, vhi, seed);
+    CK(cudaGetLastError());
+    c->launches += 1;
+    if (!wants_blobs(rbc)) return;
+    BlobSet &bs = c->slot_host[slot];
+    bs = c->blob_cache.take(blob_key(c, rbc, seed));
+    if (bs.blobs.empty()) return;
+    SlotBlobs &d = c->slot_dev[slot];
+    d.blobs.ensure(bs.blobs.size());
+    d.first.ensure(bs.first.size());
+    d.list.ensure(std::max<size_t>(bs.list.size(), 1));
+    CK(cudaMemcpyAsync(d.blobs.p, bs.blobs.data(), bs.blobs.size() * sizeof(Blob), cudaMemcpyHostToDevice,
+                       c->stream));
+    CK(cudaMemcpyAsync(d.first.p, bs.first.data(), bs.first.size() * sizeof(int), cudaMemcpyHostToDevice,
+                       c->stream));
+    if (!bs.list.empty())
+        CK(cudaMemcpyAsync(d.list.p, bs.list.data(), bs.list.size() * sizeof(int), cudaMemcpyHostToDevice,
+                           c->stream));
+    rbc_blobs_kernel<<<grid_blocks(c->vol), 256, 0, c->stream>>>(dst, c->nzz, c->nxx, c->nyy, c->ldz, c->g.nb,
+                                                                 c->g.dh, d.blobs.p, d.first.p, d.list.p, bs.nbz,
+                                                                 bs.nbx, bs.nby, bs.bin, vlo, vhi);
+    CK(cudaGetLastError());
+    c->launches += 1;
+}
+
+// Capacity for n velocity slots; slot 0 (the current model) is kept.
+void grow_velocity_slots(fwi_ctx *c, int n)
+{
+    const size_t want = (size_t)n * c->vol;
+    if (c->vp.n >= want) return;
+    DevBuf<float> nv;
+    nv.ensure(want);
+    cudaError_t e = cudaMemcpyAsync(nv.p, c->vp.p, c->vol * sizeof(float), cudaMemcpyDeviceToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+        nv.release();
+        CK(e);
+    }
+    c->vp.release();
+    c->vp = nv;
+    ++c->generation;
+}
+
+// Per-shot random pads of one batch (shots ids[0..n)), then the blob sets
+// of the next batch's shots start building on host threads.
+void shot_pads(fwi_ctx *c, const int *ids, int n, const int *next, int n_next)
+{
+    for (int k = 0; k < n; ++k) pad_slot(c, &c->shot_rbc_params, c->shot_rbc_seed + (uint64_t)ids[k], c->vel_slots > 1 ? k : 0);
+    if (wants_blobs(&c->shot_rbc_params))
+        for (int k = 0; k < n_next; ++k)
+            c->blob_cache.prefetch(blob_key(c, &c->shot_rbc_params, c->shot_rbc_seed + (uint64_t)next[k]));
+    // synchronises the stream: the slots' host blob copies outlive their uploads
+    check_cfl(c, c->vel_slots > 1 ? n : 1);
 }
 
 }  // namespace
@@ -1166,10 +1323,8 @@ int fwi_destroy(fwi_ctx *c)
     c->ubits.release();
     c->post.release();
     c->stage.release();
-    c->blob_dev.release();
-    c->bin_first.release();
-    c->bin_list.release();
-    if (c->blobs_next.valid()) c->blobs_next.wait();
+    for (auto &d : c->slot_dev) d.release();
+    c->blob_cache.drain();
     for (auto &e : c->ev)
         if (e) cudaEventDestroy(e);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -1271,67 +1426,59 @@ int fwi_apply_random_boundary(fwi_ctx *c, const fwi_rbc *rbc, uint64_t seed)
     if (!c || !rbc) return FWI_ERR_ARG;
     return guarded(c, [&] {
         if (!c->have_vp) fail(FWI_ERR_STATE, "no velocity model set");
-        if (rbc->kind != 0 && rbc->kind != 1) fail(FWI_ERR_ARG, "unknown random boundary kind %d", rbc->kind);
-        const double cap = (rbc->cfl_cap > 0 ? rbc->cfl_cap : 0.98) * stability_velocity(c->g.dh, c->p.dt);
-        float vlo, vhi;
-        if (rbc->kind == 0) {
-            vlo = c->vmin - rbc->varVp;
-            vhi = (float)std::min<double>(c->vmax + rbc->varVp, cap);
-            vlo = std::max(vlo, 0.05f * c->vmin);
-        } else {
-            vlo = 0.05f * c->vmin;
-            vhi = (float)cap;
-        }
-        // always start from the clean padded model (no drift between shots)
-        CK(cudaMemcpyAsync(c->vp.p, c->vp_clean.p, c->vol * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
-        rbc_background_kernel<<<grid_blocks(c->vol), 256, 0, c->stream>>>(
-            c->vp.p, c->nzz, c->nxx, c->nyy, c->ldz, c->g.nb, rbc->kind, rbc->ratio, rbc->varVp, vlo, vhi, seed);
-        CK(cudaGetLastError());
-        c->launches += 1;
-        if (rbc->kind == 0 && rbc->ratio > 0 && rbc->varVp > 0) {
-            const float dh = c->g.dh;
-            BlobKey key;
-            key.seed = seed;
-            key.xm = (c->nxx - 1) * dh;
-            key.ym = (c->nyy - 1) * dh;
-            key.zm = (c->nzz - 1) * dh;
-            key.ratio = rbc->ratio;
-            key.varVp = rbc->varVp;
-            key.fnb = c->g.nb * dh;
-            // the previous call started this seed's blob set on a host thread
-            // when shots come with consecutive seeds; otherwise build it now
-            if (c->blobs_next.valid() && c->blobs_next_key == key) {
-                c->blobs_now = c->blobs_next.get();
-            } else {
-                if (c->blobs_next.valid()) c->blobs_next.wait();
-                c->blobs_now = make_blobs(key);
-            }
-            BlobKey next = key;
-            next.seed = seed + 1;
-            c->blobs_next_key = next;
-            c->blobs_next = std::async(std::launch::async, make_blobs, next);
-            const BlobSet &bs = c->blobs_now;
-            if (!bs.blobs.empty()) {
-                c->blob_dev.ensure(bs.blobs.size());
-                c->bin_first.ensure(bs.first.size());
-                c->bin_list.ensure(std::max<size_t>(bs.list.size(), 1));
-                CK(cudaMemcpyAsync(c->blob_dev.p, bs.blobs.data(), bs.blobs.size() * sizeof(Blob),
-                                   cudaMemcpyHostToDevice, c->stream));
-                CK(cudaMemcpyAsync(c->bin_first.p, bs.first.data(), bs.first.size() * sizeof(int),
-                                   cudaMemcpyHostToDevice, c->stream));
-                if (!bs.list.empty())
-                    CK(cudaMemcpyAsync(c->bin_list.p, bs.list.data(), bs.list.size() * sizeof(int),
-                                       cudaMemcpyHostToDevice, c->stream));
-                rbc_blobs_kernel<<<grid_blocks(c->vol), 256, 0, c->stream>>>(
-                    c->vp.p, c->nzz, c->nxx, c->nyy, c->ldz, c->g.nb, dh, c->blob_dev.p, c->bin_first.p,
-                    c->bin_list.p, bs.nbz, bs.nbx, bs.nby, bs.bin, vlo, vhi);
-                CK(cudaGetLastError());
-                c->launches += 1;
-            }
-        }
-        // check_cfl synchronises the stream, so the host vectors behind the
-        // uploads above stay valid until the copies are done
+        check_rbc(rbc);
+        pad_slot(c, rbc, seed, 0);
+        // shots that come with consecutive seeds find their blob set ready
+        if (wants_blobs(rbc)) c->blob_cache.prefetch(blob_key(c, rbc, seed + 1));
+        // synchronises the stream: the host blob copy outlives its upload
         check_cfl(c);
+    });
+}
+
+int fwi_set_shot_random_boundary(fwi_ctx *c, const fwi_rbc *rbc, uint64_t base_seed)
+{
+    if (!c) return FWI_ERR_ARG;
+    return guarded(c, [&] {
+        if (!rbc) {
+            if (c->shot_rbc && c->have_vp) {
+                CK(cudaMemcpyAsync(c->vp.p, c->vp_clean.p, c->vol * sizeof(float), cudaMemcpyDeviceToDevice,
+                                   c->stream));
+                CK(cudaStreamSynchronize(c->stream));
+            }
+            c->shot_rbc = false;
+            c->vel_slots = 1;
+            return;
+        }
+        if (!c->have_vp) fail(FWI_ERR_STATE, "no velocity model set");
+        check_rbc(rbc);
+        grow_velocity_slots(c, c->B);
+        c->shot_rbc = true;
+        c->shot_rbc_params = *rbc;
+        c->shot_rbc_seed = base_seed;
+        c->vel_slots = c->B;
+    });
+}
+
+int fwi_random_boundary_recipe(fwi_ctx *c, const fwi_rbc *rbc, uint64_t seed, float *vlo, float *vhi,
+                               float *blobs, int cap, int *nblobs)
+{
+    if (!c || !rbc || cap < 0 || (cap > 0 && !blobs)) return FWI_ERR_ARG;
+    return guarded(c, [&] {
+        if (!c->have_vp) fail(FWI_ERR_STATE, "no velocity model set");
+        check_rbc(rbc);
+        float lo, hi;
+        rbc_bounds(c, rbc, lo, hi);
+        if (vlo) *vlo = lo;
+        if (vhi) *vhi = hi;
+        BlobSet bs;
+        if (wants_blobs(rbc)) bs = make_blobs(blob_key(c, rbc, seed));
+        const int n = (int)bs.blobs.size();
+        if (nblobs) *nblobs = n;
+        for (int q = 0; q < std::min(n, cap); ++q) {
+            const Blob &b = bs.blobs[q];
+            const float v[5] = {b.x, b.y, b.z, b.r, b.amp};
+            memcpy(blobs + 5 * (size_t)q, v, sizeof v);
+        }
     });
 }
 

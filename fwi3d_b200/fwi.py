@@ -1,14 +1,30 @@
-"""FWI driver over the C ABI: misfit, gradient, parabolic line search and the
-learned-step accept rule.
+"""FWI driver over the C ABI: misfit, gradient, line search and the
+learned-step accept rule, shot-parallel over ranks.
 
-The plain method is the reference's (src/inversion/inversion.cu:206-453):
+The plain method is the reference's (src/inversion/inversion.cu:115-362):
 illumination-scaled, depth-masked, -d2/dz2-filtered gradient normalised by
-max|g|; parabola through the misfits of the slowness-squared steps 0,
-0.02 dm and 0.05 dm (dm = 1/vmin^2 - 1/vmax^2); m <- m - step g.  This driver
-uses the fixed behaviour (updated model used for the next gradient, fresh
-illumination per gradient, d2/dy2 kept, source removed in the rebuild, step
-bounded to [0, 8 x 0.05 dm], every model kept below the leapfrog stability
-limit); inversion.exe keeps the reference's quirks for drop-in parity.
+max|g|, a step on the slowness-squared model m = 1/v^2 with trial steps
+0.02 dm and 0.05 dm (dm = 1/vmin^2 - 1/vmax^2) and a parabola through the
+square roots of the misfits, then m <- m - step g.  This driver keeps the
+fixed behaviour (updated model used for the next gradient, fresh
+illumination per gradient, d2/dy2 kept, source removed in the rebuild, a new
+random boundary per shot) and makes the step search measured:
+
+  - every candidate step's misfit is computed, never predicted;
+  - while the misfit still falls at the largest step tried, the step doubles
+    (the reference stops at its two trials and extrapolates the parabola
+    without bound, inversion.cu:331-347);
+  - the parabola's vertex through the best step and its neighbours is then
+    measured too, and the best measured candidate is taken;
+  - every step stays within STEP_BOUND x 0.05 dm and the MAX_DV trust region,
+    and every model below the leapfrog stability limit.
+
+inversion.exe keeps the reference's quirks for drop-in parity.
+
+Shots are dealt to ranks (torch.distributed; one process per GPU): each rank
+models and back-propagates its own shots, the FP64 misfit is summed over
+ranks, and the padded gradient and illumination are summed before the
+post-processing, so every rank takes the same steps.
 
 Observed, modelled and residual data stay on the GPU (torch tensors used as
 device buffers); every propagation, reduction and post-processing step runs
@@ -16,23 +32,21 @@ in libfwi3d.so.  Misfits are FP64 sums of squares.
 """
 from __future__ import annotations
 
+import hashlib
 import time
 from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import lib
+from . import lib, shots
 from .synth import Workload
 
-# Largest step as a multiple of the largest trial step: the reference's parabola
-# vertex is unbounded and can leave the physical range (inversion.cu:400-403).
+# Largest step as a multiple of the 0.05 dm trial step (inversion.exe uses the
+# same bound): the reference's parabola vertex is unbounded and can leave the
+# physical range (inversion.cu:331-347).
 STEP_BOUND = 8.0
 # Trust region of the plain update: no cell's velocity changes by more than
-# this fraction in one iteration.  The largest trial step (0.05 dm) changes
-# the fastest cells of a 1500-4500 m/s model by about 15 %; a step the
-# parabola extrapolates to the bound can double them, and where the clip to
-# the velocity bounds catches them the model error grows while the misfit
-# still falls.
+# this fraction in one iteration.
 MAX_DV = 0.2
 
 
@@ -55,26 +69,99 @@ def stability_velocity(dh: float, dt: float) -> float:
     return 2.0 / np.sqrt(3.0 * s) * dh / dt
 
 
-class Fwi:
-    """One inversion problem: geometry, observed data, two library contexts."""
+def model_key(v) -> bytes:
+    """Identity of a model's exact FP32 values."""
+    return hashlib.blake2b(np.ascontiguousarray(v, np.float32).tobytes(), digest_size=16).digest()
 
-    def __init__(self, w: Workload, opts: FwiOptions | None = None, obs=None):
+
+def parabola_vertex(a, r):
+    """Vertex of the parabola through (a_i, r_i), i = 0..2 (the reference's
+    formula, inversion.cu:331-347); None when it is not a minimum."""
+    num = (a[1] ** 2 - a[2] ** 2) * r[0] + (a[2] ** 2 - a[0] ** 2) * r[1] + (a[0] ** 2 - a[1] ** 2) * r[2]
+    den = (a[1] - a[2]) * r[0] + (a[2] - a[0]) * r[1] + (a[0] - a[1]) * r[2]
+    # positive second divided difference: a minimum
+    convex = (r[2] - r[1]) / (a[2] - a[1]) > (r[1] - r[0]) / (a[1] - a[0])
+    if den == 0 or not convex:
+        return None
+    return 0.5 * num / den
+
+
+def search_step(misfit, trial, f0, a1, a2, cap):
+    """Measured step search.  misfit(alpha) returns the misfit of trial step
+    alpha; steps are capped at `cap`.  Returns (best step, its misfit), with
+    (0, f0) when no candidate lowers the misfit."""
+    a, f = [0.0], [f0]
+
+    def measure(alpha):
+        if alpha <= 0 or any(abs(alpha - x) <= 1e-12 * max(alpha, x) for x in a):
+            return
+        a.append(alpha)
+        f.append(misfit(alpha))
+
+    measure(min(a1, cap))
+    measure(min(a2, cap))
+    # expand while the misfit still falls at the largest step
+    while len(a) > 2 and f[-1] < f[-2] and a[-1] < cap * (1 - 1e-12):
+        measure(min(2.0 * a[-1], cap))
+    # shrink when even the smallest trial is worse than no step
+    for _ in range(2):
+        if int(np.argmin(f)) != 0:
+            break
+        measure(0.25 * min(x for x in a if x > 0))
+    order = np.argsort(a)
+    a, f = [a[i] for i in order], [f[i] for i in order]
+    k = int(np.argmin(f))
+    if 0 < k < len(a) - 1:
+        v = parabola_vertex(a[k - 1:k + 2], np.sqrt(f[k - 1:k + 2]))
+        if v is not None and a[k - 1] < v < a[k + 1]:
+            measure(min(v, cap))
+    k = int(np.argmin(f))
+    return (a[k], f[k]) if k else (0.0, f0)
+
+
+class Fwi:
+    """One inversion problem: geometry, observed data of this rank's shots,
+    two library contexts (Cerjan boundary for the data, random boundary for
+    the gradient).
+
+    world/rank default to torch.distributed's when it is initialised.
+    `contexts` replaces the two library contexts by objects with the same
+    methods (the CPU tests of the cross-rank logic), with buffers on `device`."""
+
+    def __init__(self, w: Workload, opts: FwiOptions | None = None, obs=None, world=None, rank=None,
+                 contexts=None, device="cuda"):
         import torch
         self.torch = torch
         self.w, self.o = w, opts or FwiOptions()
-        flags = (lib.FLAG_GRAD_DY | lib.FLAG_SUBTRACT_SOURCE) if self.o.fixes else 0
-        self.abc = lib.Context(w.nz, w.nx, w.ny, w.nb, w.dh, w.nt, w.dt, w.fmax, lib.BOUNDARY_ABC,
-                               w.abc_factor, self.o.batch, 0)
-        self.rbc = lib.Context(w.nz, w.nx, w.ny, w.nb, w.dh, w.nt, w.dt, w.fmax, lib.BOUNDARY_RBC, 0.0,
-                               self.o.batch, flags)
+        self.device = device
+        if world is None:
+            import torch.distributed as dist
+            ok = dist.is_available() and dist.is_initialized()
+            world, rank = (dist.get_world_size(), dist.get_rank()) if ok else (1, 0)
+        self.world, self.rank = world, rank
+        if contexts is None:
+            flags = (lib.FLAG_GRAD_DY | lib.FLAG_SUBTRACT_SOURCE) if self.o.fixes else 0
+            contexts = (lib.Context(w.nz, w.nx, w.ny, w.nb, w.dh, w.nt, w.dt, w.fmax, lib.BOUNDARY_ABC,
+                                    w.abc_factor, self.o.batch, 0),
+                        lib.Context(w.nz, w.nx, w.ny, w.nb, w.dh, w.nt, w.dt, w.fmax, lib.BOUNDARY_RBC, 0.0,
+                                    self.o.batch, flags))
+        self.abc, self.rbc = contexts
         for c in (self.abc, self.rbc):
             c.set_geometry(w.src, w.rec, w.rec_first, w.rec_count)
         self.nshot = len(w.src)
-        counts = [self.abc.shot_nrec(s) * w.nt for s in range(self.nshot)]
+        self.mine = shots.partition(self.nshot, world, rank)
+        counts = [self.abc.shot_nrec(s) * w.nt for s in self.mine]
         self.offset = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
-        n = int(self.offset[-1])
-        self.cal = torch.empty(n, device="cuda", dtype=torch.float32)
-        self.res = torch.empty(n, device="cuda", dtype=torch.float32)
+        n = max(int(self.offset[-1]), 1)
+        self.cal = torch.empty(n, device=device, dtype=torch.float32)
+        self.res = torch.empty(n, device=device, dtype=torch.float32)      # residual of _res_key
+        self.res_tmp = torch.empty(n, device=device, dtype=torch.float32)  # residual of _tmp_key
+        self._res_key = self._tmp_key = None
+        self._known = {}
+        self.acc = None
+        if world > 1:
+            cells = self.rbc.nzz * self.rbc.nxx * self.rbc.nyy
+            self.acc = (torch.empty(cells, device=device), torch.empty(cells, device=device))
         self.obs = obs if obs is not None else self.model(w.vp)
         self.evals = 0
         self.gradients = 0
@@ -82,38 +169,67 @@ class Fwi:
 
     # -- building blocks ------------------------------------------------------
     def _batches(self):
+        """(position in self.mine, shot ids) of each launch."""
         B = self.o.batch
-        return [list(range(s, min(s + B, self.nshot))) for s in range(0, self.nshot, B)]
+        return [(i, self.mine[i:i + B]) for i in range(0, len(self.mine), B)]
+
+    def _ptr(self, buf, i):
+        return buf.data_ptr() + 4 * int(self.offset[i])
 
     def model(self, v):
-        """Seismograms of every shot for velocity v (device tensor)."""
-        out = self.torch.empty(int(self.offset[-1]), device="cuda", dtype=self.torch.float32)
+        """Seismograms of this rank's shots for velocity v (device tensor)."""
+        out = self.torch.empty(max(int(self.offset[-1]), 1), device=self.device, dtype=self.torch.float32)
         self.abc.set_velocity(v)
-        self.torch.cuda.synchronize()
-        for b in self._batches():
-            self.abc.model_shots_dev(b, out.data_ptr() + 4 * int(self.offset[b[0]]))
+        if self.device == "cuda":
+            self.torch.cuda.synchronize()
+        for i, b in self._batches():
+            self.abc.model_shots_dev(b, self._ptr(out, i))
         return out
 
     def misfit(self, v) -> float:
-        """sum (obs - cal)^2 over every shot and sample (FP64)."""
+        """sum (obs - cal)^2 over every shot of every rank (FP64).  The
+        residual stays in res_tmp until adopt(v) keeps it."""
         self.abc.set_velocity(v)
-        for b in self._batches():
-            self.abc.model_shots_dev(b, self.cal.data_ptr() + 4 * int(self.offset[b[0]]))
+        for i, b in self._batches():
+            self.abc.model_shots_dev(b, self._ptr(self.cal, i))
         self.evals += 1
-        return self.abc.residual_dev(self.obs.data_ptr(), self.cal.data_ptr(), int(self.offset[-1]),
-                                     self.res.data_ptr())
+        local = self.abc.residual_dev(self.obs.data_ptr(), self.cal.data_ptr(), int(self.offset[-1]),
+                                      self.res_tmp.data_ptr()) if len(self.mine) else 0.0
+        f = shots.misfit_across_ranks(local)
+        self._tmp_key = model_key(v)
+        self._known[self._tmp_key] = f
+        return f
+
+    def adopt(self, v):
+        """Keep the residual of v (the model just evaluated) for its gradient."""
+        k = model_key(v)
+        if self._tmp_key == k:
+            self.res, self.res_tmp = self.res_tmp, self.res
+            self._res_key, self._tmp_key = k, None
+
+    def known_misfit(self, v) -> float:
+        k = model_key(v)
+        return self._known[k] if k in self._known else self.misfit(v)
 
     def gradient(self, v):
         """Misfit of v, then the gradient: returns (post-processed gradient,
         raw cropped gradient, cropped illumination, misfit)."""
-        f = self.misfit(v)
+        k = model_key(v)
+        if self._res_key == k and k in self._known:
+            f = self._known[k]
+        else:
+            f = self.misfit(v)
+            self.adopt(v)
+        self._known = {k: f}
         self.rbc.reset_accumulators()
         self.rbc.set_velocity(v)
-        # the random pads depend only on how many gradients came before, so two
-        # runs that take the same steps see the same pads
-        for k, b in enumerate(self._batches()):
-            self.rbc.apply_random_boundary(seed=self.o.seed + 7919 * self.gradients + k, **self.o.rbc)
-            self.rbc.gradient_shots_dev(b, self.res.data_ptr() + 4 * int(self.offset[b[0]]))
+        # shot s propagates through the pad of seed base + s: the pads depend
+        # only on how many gradients came before, not on ranks or batches
+        self.rbc.set_shot_random_boundary(base_seed=self.o.seed + 7919 * self.gradients, **self.o.rbc)
+        for i, b in self._batches():
+            self.rbc.gradient_shots_dev(b, self._ptr(self.res, i))
+        if self.acc is not None:
+            shots.reduce_context_accumulators(self.rbc, *self.acc)
         self.gradients += 1
         g, _ = self.rbc.gradient_post(self.o.zmask)
         raw, ill = self.rbc.get_accumulators()
@@ -121,43 +237,44 @@ class Fwi:
 
     # -- plain line search ----------------------------------------------------
     def line_search(self, v, g, f0, dm):
-        """Bounded parabolic step on m = 1/v^2, within the MAX_DV trust
-        region.  Returns (new velocity, step, the parabola's predicted misfit
-        at the step)."""
+        """Measured step on m = 1/v^2 along -g (search_step), within
+        STEP_BOUND x 0.05 dm and the MAX_DV trust region.  Returns (new
+        velocity, step, its measured misfit); the new model's residual is kept
+        for its gradient."""
         if not (dm > 0) or not np.all(np.isfinite(g)) or not np.any(g):
             return v, 0.0, f0
         m = 1.0 / (v.astype(np.float64) ** 2)
         g64 = np.asarray(g, np.float64)
-        a = np.array([0.0, 0.02 * dm, 0.05 * dm])
         lo, hi = self.vbounds
-
         def trial(alpha):
             # FP64 throughout, whatever the type of alpha: a Python float times
             # an FP32 array would round the product to FP32, so the same step
             # would give a slightly different model each way it is written
             return np.clip(1.0 / np.sqrt(np.maximum(m - float(alpha) * g64, 1e-12)), lo, hi).astype(np.float32)
-        f = np.array([f0, self.misfit(trial(a[1])), self.misfit(trial(a[2]))])
-        # the reference fits the parabola to sqrt(sum res^2) (inversion.cu:390-403)
-        r = np.sqrt(f)
-        num = (a[1] ** 2 - a[2] ** 2) * r[0] + (a[2] ** 2 - a[0] ** 2) * r[1] + (a[0] ** 2 - a[1] ** 2) * r[2]
-        den = (a[1] - a[2]) * r[0] + (a[2] - a[0]) * r[1] + (a[0] - a[1]) * r[2]
-        step = 0.5 * num / den if den != 0 else 0.0
-        convex = (r[2] - r[1]) / (a[2] - a[1]) > (r[1] - r[0]) / (a[1] - a[0])
-        if not convex or not step > 0:
-            step = float(a[int(np.argmin(r))])
-        step = min(step, STEP_BOUND * a[2])
-        # the velocity change grows about linearly with the step: shrink it
-        # until the largest relative change is within MAX_DV
-        v64 = v.astype(np.float64)
-        for _ in range(4):
-            rel = float(np.max(np.abs(trial(step).astype(np.float64) / v64 - 1.0))) if step > 0 else 0.0
-            if rel <= MAX_DV * (1 + 1e-6):
-                break
-            step *= MAX_DV / rel
-        # the parabola through the trials, evaluated at the step (Lagrange form)
-        lag = sum(r[i] * np.prod([(step - a[j]) / (a[i] - a[j]) for j in range(3) if j != i]) for i in range(3))
-        pred = float(f[1] if step == a[1] else f[2] if step == a[2] else f[0] if step == 0 else max(lag, 0.0) ** 2)
-        return trial(step), float(step), pred
+
+        # largest step within the trust region, cell by cell in closed form:
+        # v'/v = sqrt(m / (m - alpha g)) stays in [1 - MAX_DV, 1 + MAX_DV] for
+        # alpha <= m (1 - 1/(1 + MAX_DV)^2) / g where g > 0 and
+        # alpha <= m (1/(1 - MAX_DV)^2 - 1) / |g| where g < 0 (the clip to the
+        # velocity bounds only shrinks a change)
+        with np.errstate(divide="ignore"):
+            lim = np.where(g64 > 0, m * (1.0 - 1.0 / (1.0 + MAX_DV) ** 2) / g64,
+                           np.where(g64 < 0, m * (1.0 / (1.0 - MAX_DV) ** 2 - 1.0) / -g64, np.inf))
+        cap = min(STEP_BOUND * 0.05 * dm, float(np.min(lim)))
+        best = {}
+
+        def f_of(alpha):
+            vt = trial(alpha)
+            f = self.misfit(vt)
+            if f < best.get("f", f0):
+                best["f"] = f
+                self.adopt(vt)
+            return f
+
+        step, f = search_step(f_of, trial, f0, 0.02 * dm, 0.05 * dm, cap)
+        if step == 0.0:
+            return v, 0.0, f0
+        return trial(step), float(step), f
 
 
 def rms(v, ref) -> float:
@@ -167,8 +284,9 @@ def rms(v, ref) -> float:
 def run(prob: Fwi, v0, iterations: int, learned=None, log=print):
     """Run `iterations` updates from v0.  With `learned` (a callable mapping
     (raw gradient, velocity, illumination) to a velocity update), each
-    iteration also evaluates v + learned(...) and keeps it only when its misfit
-    is at most the plain step's.  Returns (final velocity, history)."""
+    iteration also measures the misfit of v + learned(...) and keeps it only
+    when it is at most the plain step's measured misfit.  Returns (final
+    velocity, history)."""
     w = prob.w
     vmin, vmax = float(v0.min()), float(v0.max())
     dm = 1.0 / vmin ** 2 - 1.0 / vmax ** 2
@@ -191,11 +309,13 @@ def run(prob: Fwi, v0, iterations: int, learned=None, log=print):
             f_l = prob.misfit(v_l)
             if f_l <= f_plain:
                 v_next, choice = v_l, "learned"
+                prob.adopt(v_l)
             hist[-1].update(f_learned=f_l)
-        hist[-1].update(step=step, f_plain_pred=f_plain, choice=choice)
+        hist[-1].update(step=step, f_plain=f_plain, choice=choice, evals=prob.evals)
         log(f"iter {it}: misfit {f0:.6e} rms {hist[-1]['rms']:.2f} step {step:.3e} -> {choice}")
         v = v_next
-    f = prob.misfit(v)
-    hist.append(dict(iteration=iterations, misfit=f, rms=rms(v, w.vp), time=time.perf_counter() - t0))
+    f = prob.known_misfit(v)
+    hist.append(dict(iteration=iterations, misfit=f, rms=rms(v, w.vp), time=time.perf_counter() - t0,
+                     evals=prob.evals))
     log(f"final: misfit {f:.6e} rms {hist[-1]['rms']:.2f} after {hist[-1]['time']:.1f} s")
     return v, hist

@@ -15,7 +15,8 @@
 // By default (b200_fixes = 1) the loop corrects the reference's quirks: it
 // uploads the updated model, zeroes the illumination per gradient, keeps
 // d2/dy2, removes the source in the rebuild and bounds the line-search step to
-// [0, 4 x the largest trial step].  b200_fixes = 0 reproduces the reference
+// [0, 8 x the largest trial step] (the bound of the Python driver, fwi.py).
+// b200_fixes = 0 reproduces the reference
 // for parity, quirks included: the device model keeps the 0.05 dm trial model
 // after the line search, the illumination accumulates over every gradient,
 // there is no d2/dy2 term and no source removal, and the step is unbounded
@@ -26,6 +27,10 @@
 #include "workflow.hpp"
 
 namespace {
+
+// Largest line-search step as a multiple of the 0.05 dm trial step (the same
+// bound as fwi.STEP_BOUND).
+constexpr float kStepBound = 8.0f;
 
 struct Inversion {
     std::string pf;
@@ -112,12 +117,12 @@ struct Inversion {
             // The reference extrapolates the parabola without bound; with a
             // misfit that falls almost linearly over [0, a2] its vertex lands far
             // outside the bracket and the model leaves the physical range.  Keep
-            // the step in [0, 4 a2], and take the best trial step when the
+            // the step in [0, 8 a2], and take the best trial step when the
             // parabola is not convex.
             const float slope01 = (f1 - f0) / (a1 - a0), slope12 = (f2 - f1) / (a2 - a1);
             const bool convex = slope12 > slope01;  // positive second divided difference
             if (!convex || !(step > 0)) step = f2 < f1 ? (f2 < f0 ? a2 : 0.0f) : (f1 < f0 ? a1 : 0.0f);
-            step = std::min(step, 4.0f * a2);
+            step = std::min(step, kStepBound * a2);
         }
         std::vector<float> v(npts);
 #pragma omp parallel for

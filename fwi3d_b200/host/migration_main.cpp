@@ -30,20 +30,28 @@ int main(int argc, char **argv)
         const int seed = fwh::opt_i(pf, "b200_seed", 1);
         const int flags = fwh::opt_i(pf, "b200_fixes", 1) ? FWI_FLAG_SUBTRACT_SOURCE : 0;
         const int nb = fwh::pad_cells(length, m.dh);
-        fwi_ctx *ctx = fwh::make_context(m, nb, FWI_BOUNDARY_RBC, 0.0f, 1, flags);
+        fwi_ctx *ctx = fwh::make_context(m, nb, FWI_BOUNDARY_RBC, 0.0f, batch, flags);
         fwh::check(fwi_set_velocity(ctx, m.vp.data()), ctx, "fwi_set_velocity");
         std::cout << fwh::banner("Reverse Time Migration");
-        (void)batch;  // every shot has its own random boundary: one shot per pass
 
         fwh::Clock clock;
         const size_t per_shot = (size_t)m.nt * m.rec.n;
-        std::vector<float> data(per_shot);
+        // every shot gets its own random boundary (seed b200_seed + s), built
+        // per batch slot, so `batch` shots with different pads share a launch
         const fwi_rbc rbc{0, ratio, varVp, 0.98f};
-        for (int s = 0; s < m.src.n; ++s) {
-            std::cout << "Running shot " << s + 1 << " of " << m.src.n << " in total\n";
-            fwh::check(fwi_apply_random_boundary(ctx, &rbc, (uint64_t)(seed + s)), ctx, "random boundary");
-            fwh::read_binary(in_folder + in_prefix + std::to_string(s + 1) + ".bin", data.data(), per_shot);
-            fwh::check(fwi_rtm_shots(ctx, &s, 1, data.data()), ctx, "fwi_rtm_shots");
+        fwh::check(fwi_set_shot_random_boundary(ctx, &rbc, (uint64_t)seed), ctx, "random boundary");
+        std::vector<float> data(per_shot * batch);
+        std::vector<int> ids(batch);
+        for (int s0 = 0; s0 < m.src.n; s0 += batch) {
+            const int n = std::min(batch, m.src.n - s0);
+            for (int k = 0; k < n; ++k) {
+                const int s = s0 + k;
+                std::cout << "Running shot " << s + 1 << " of " << m.src.n << " in total\n";
+                ids[k] = s;
+                fwh::read_binary(in_folder + in_prefix + std::to_string(s + 1) + ".bin", data.data() + k * per_shot,
+                                 per_shot);
+            }
+            fwh::check(fwi_rtm_shots(ctx, ids.data(), n, data.data()), ctx, "fwi_rtm_shots");
         }
         const double secs = clock.seconds();
         std::vector<float> image((size_t)m.nz * m.nx * m.ny);

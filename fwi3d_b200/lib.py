@@ -50,6 +50,8 @@ SIGNATURES = {
     "fwi_set_padded_velocity": (_i, [_p, _fp]),
     "fwi_get_padded_velocity": (_i, [_p, _fp]),
     "fwi_apply_random_boundary": (_i, [_p, _p, C.c_uint64]),
+    "fwi_set_shot_random_boundary": (_i, [_p, _p, C.c_uint64]),
+    "fwi_random_boundary_recipe": (_i, [_p, _p, C.c_uint64, _fp, _fp, _fp, _i, _ip]),
     "fwi_set_geometry": (_i, [_p, _i, _fp, _fp, _fp, _i, _fp, _fp, _fp, _ip, _ip]),
     "fwi_shot_nrec": (_i, [_p, _i, _ip]),
     "fwi_model_shots": (_i, [_p, _ip, _i, _fp]),
@@ -224,6 +226,30 @@ class Context:
     def apply_random_boundary(self, kind=0, ratio=100.0, varVp=1000.0, cfl_cap=0.98, seed=1):
         r = FwiRbc(kind, ratio, varVp, cfl_cap)
         self._check(self.lib.fwi_apply_random_boundary(self.h, C.byref(r), C.c_uint64(seed)))
+
+    def set_shot_random_boundary(self, kind=0, ratio=100.0, varVp=1000.0, cfl_cap=0.98, base_seed=1):
+        """From now on shot s propagates through the random pad of seed
+        base_seed + s, rebuilt for every batch (one velocity slot per batch
+        slot)."""
+        r = FwiRbc(kind, ratio, varVp, cfl_cap)
+        self._check(self.lib.fwi_set_shot_random_boundary(self.h, C.byref(r), C.c_uint64(base_seed)))
+
+    def clear_shot_random_boundary(self):
+        """Back to one shared velocity: the clean padded model."""
+        self._check(self.lib.fwi_set_shot_random_boundary(self.h, None, C.c_uint64(0)))
+
+    def random_boundary_recipe(self, kind=0, ratio=100.0, varVp=1000.0, cfl_cap=0.98, seed=1):
+        """(vlo, vhi, blobs) of one seed: the clamp bounds and an (n, 5) array
+        of blobs (x, y, z, r, signed amplitude) in the order they are added."""
+        r = FwiRbc(kind, ratio, varVp, cfl_cap)
+        lo, hi, n = C.c_float(), C.c_float(), C.c_int()
+        self._check(self.lib.fwi_random_boundary_recipe(self.h, C.byref(r), C.c_uint64(seed), C.byref(lo),
+                                                        C.byref(hi), None, 0, C.byref(n)))
+        blobs = np.zeros((n.value, 5), np.float32)
+        if n.value:
+            self._check(self.lib.fwi_random_boundary_recipe(self.h, C.byref(r), C.c_uint64(seed), None, None,
+                                                            _fptr(blobs), n.value, C.byref(n)))
+        return lo.value, hi.value, blobs
 
     # -- geometry -----------------------------------------------------------
     def set_geometry(self, src_xyz, rec_xyz, rec_first=None, rec_count=None):

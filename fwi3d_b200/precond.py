@@ -1,11 +1,14 @@
 """Learned gradient preconditioner: data, training and use inside FWI.
 
 Pairs come from the project's own FWI on seeded random models (synth.cnn_128):
-inputs are the raw gradient, the velocity and the illumination of the start
-model's first gradient, the target is true - start velocity.  The network is
-fwi_cnn_* in libfwi3d.so (BF16 tensor cores, FP32 accumulation, FP32 Adam).
+inputs are the raw gradient, the velocity and the illumination at a model v,
+the target is true - v.  Each model gives pairs at the smoothed start model
+and at a partly corrected model v = start + s (true - start), s drawn from
+[0.3, 0.8), so that at a later iterate the network predicts the remaining
+correction instead of the whole one again.  The network is fwi_cnn_* in
+libfwi3d.so (BF16 tensor cores, FP32 accumulation, FP32 Adam).
 
-    python -m fwi3d_b200.precond pipeline --models 0:136 --weights W.npz --report R.json
+    python -m fwi3d_b200.precond pipeline --models 0:200 --weights W.npz --report R.json
     python -m fwi3d_b200.precond compare --weights W.npz --iterations 5 --out C.json
     python -m fwi3d_b200.precond time --n 128 --steps 20 --warmup 2
 
@@ -38,16 +41,28 @@ def features(raw, v, ill, zmask_cells=0):
     return np.stack([g, vv, il]).astype(np.float32)
 
 
-def pair_from(w: synth.Workload, batch: int, seed: int):
-    prob = fwi.Fwi(w, fwi.FwiOptions(batch=batch, seed=seed, zmask=w.zmask, rbc=w.rbc))
-    _, raw, ill, f = prob.gradient(w.start)
-    x = features(raw, w.start, ill, int(w.zmask / w.dh))
-    y = ((w.vp - w.start) / DV_SCALE).astype(np.float32)
+def pair_from(w: synth.Workload, batch: int, seed: int, s: float = 0.0, prob=None):
+    """(features, target, misfit) at v = start + s (true - start)."""
+    prob = prob or fwi.Fwi(w, fwi.FwiOptions(batch=batch, seed=seed, zmask=w.zmask, rbc=w.rbc))
+    v = (w.start.astype(np.float64) + s * (w.vp.astype(np.float64) - w.start)).astype(np.float32)
+    _, raw, ill, f = prob.gradient(v)
+    x = features(raw, v, ill, int(w.zmask / w.dh))
+    y = ((w.vp - v) / DV_SCALE).astype(np.float32)
     return x, y, f
 
 
-def training_pair(index: int, nt: int = 1201, batch: int = 9):
-    return pair_from(synth.cnn_128(index, nt=nt), batch, index)
+def stages(index: int) -> list[float]:
+    """The models a training model contributes pairs at: the start model and
+    one partly corrected model (seeded by the model index)."""
+    return [0.0, float(np.random.default_rng(7000 + index).uniform(0.3, 0.8))]
+
+
+def training_pairs(index: int, nt: int = 1201, batch: int = 9):
+    """Pairs of training model `index` (one FWI problem, its observed data
+    modelled once)."""
+    w = synth.cnn_128(index, nt=nt)
+    prob = fwi.Fwi(w, fwi.FwiOptions(batch=batch, seed=index, zmask=w.zmask, rbc=w.rbc))
+    return [pair_from(w, batch, index, s, prob) for s in stages(index)]
 
 
 class Learned:
@@ -115,16 +130,21 @@ def evaluate(net, xs, ys):
 
 def summarise(plain, learned):
     """Wall time for the learned run to reach the plain run's final misfit,
-    with the model RMS error of both at that point."""
+    with the model RMS error of both at that point; and the same at the plain
+    run's final model RMS error."""
     target = plain[-1]["misfit"]
     hit = next((h for h in learned if h["misfit"] <= target), None)
     out = {"plain_final_misfit": target, "plain_final_rms": plain[-1]["rms"], "plain_time": plain[-1]["time"],
+           "start_rms": plain[0]["rms"],
            "learned_final_misfit": learned[-1]["misfit"], "learned_final_rms": learned[-1]["rms"],
-           "learned_time": learned[-1]["time"],
+           "learned_time": learned[-1]["time"], "learned_max_rms": max(h["rms"] for h in learned),
            "learned_choices": [h.get("choice") for h in learned[:-1]]}
     if hit is not None:
         out.update(learned_time_to_plain_misfit=hit["time"], learned_rms_at_that_point=hit["rms"],
                    time_ratio=hit["time"] / plain[-1]["time"])
+    hit_rms = next((h for h in learned if h["rms"] <= plain[-1]["rms"]), None)
+    if hit_rms is not None:
+        out.update(learned_time_to_plain_rms=hit_rms["time"], time_ratio_at_equal_rms=hit_rms["time"] / plain[-1]["time"])
     return out
 
 
@@ -165,7 +185,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     sub = ap.add_subparsers(dest="cmd", required=True)
     pl = sub.add_parser("pipeline", help="generate pairs in memory, train, save weights and a report")
-    pl.add_argument("--models", default="0:136")
+    pl.add_argument("--models", default="0:200")
     pl.add_argument("--nt", type=int, default=1201)
     pl.add_argument("--holdout", type=int, default=8)
     pl.add_argument("--epochs", type=int, default=150)
@@ -191,18 +211,20 @@ def main(argv=None):
         t0 = time.perf_counter()
         xs, ys = [], []
         for i in range(lo, hi):
-            x, y, f = training_pair(i, a.nt)
-            xs.append(x)
-            ys.append(y)
+            for x, y, f in training_pairs(i, a.nt):
+                xs.append(x)
+                ys.append(y)
             if i % 16 == 0:
-                print(f"pair {i}: misfit {f:.4e} ({time.perf_counter() - t0:.1f} s)", flush=True)
+                print(f"model {i}: misfit {f:.4e} ({time.perf_counter() - t0:.1f} s)", flush=True)
         t_data = time.perf_counter() - t0
-        h = a.holdout
+        # hold out whole models (both of their pairs)
+        h = a.holdout * len(stages(lo))
         t1 = time.perf_counter()
         net, hist = train(xs[h:], ys[h:], epochs=a.epochs, lr=a.lr)
         t_train = time.perf_counter() - t1
         save_weights(net, a.weights)
         res = {"models": [lo, hi], "nt": a.nt, "train_pairs": len(xs) - h, "holdout_pairs": h,
+               "stages": "start model and start + s (true - start), s in [0.3, 0.8)",
                "epochs": a.epochs, "data_seconds": t_data, "train_seconds": t_train,
                "loss_first_last": [hist[0], hist[-1]], "loss_history": hist,
                "holdout_rel_error": evaluate(net, xs[:h], ys[:h]),

@@ -111,6 +111,24 @@ int fwi_get_padded_velocity(fwi_ctx *ctx, float *vp_padded);
 /* Overwrite the pad with a random boundary (replaces set_random_boundary,
  * src/modeling/modeling.cu:558-592).  Deterministic in (seed). */
 int fwi_apply_random_boundary(fwi_ctx *ctx, const fwi_rbc *rbc, uint64_t seed);
+/* A new random boundary for every shot, as the reference builds one per shot
+ * (Migration::forward_propagation, src/migration/migration.cu:49-59;
+ * Inversion::update_RBC, src/inversion/inversion.cu:204-216).  From this call
+ * on, every modeling, migration or gradient call rebuilds the velocity of each
+ * shot s of a batch from the clean padded model with the pad of seed
+ * base_seed + s.  With max_batch > 1 each batch slot reads its own velocity
+ * slot, so shots with different pads propagate in one launch and the result
+ * of a shot does not depend on the batch it runs in.  rbc == NULL turns it
+ * off and restores the clean padded model. */
+int fwi_set_shot_random_boundary(fwi_ctx *ctx, const fwi_rbc *rbc, uint64_t base_seed);
+/* The recipe behind fwi_apply_random_boundary for one seed, for checking it
+ * (no counterpart in the reference, whose pads come from clock seeds): the
+ * clamp bounds and the Gaussian blobs in the order the blob pass adds them,
+ * five floats each (x, y, z centre [m], radius [m], signed amplitude [m/s];
+ * src/modeling/modeling.cu:558-615).  At most cap blobs are written; *nblobs
+ * receives the total.  The context's state does not change. */
+int fwi_random_boundary_recipe(fwi_ctx *ctx, const fwi_rbc *rbc, uint64_t seed, float *vlo, float *vhi,
+                               float *blobs, int cap, int *nblobs);
 
 /* ---- geometry ---------------------------------------------------------- */
 /* Source and receiver coordinates in metres (SPS/RPS, src/geometry/

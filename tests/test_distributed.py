@@ -81,3 +81,136 @@ def test_two_rank_image_and_misfit_sums():
     for _, _, img, ill, misfit in out:
         assert img == want and ill == 2 * want
         assert abs(misfit - 0.1 * want) < 1e-12
+
+
+class FakeContext:
+    """Stands in for lib.Context on the CPU so that fwi.Fwi's shot partition
+    and cross-rank sums can run under gloo: a shot's 'seismogram' is a fixed
+    function of the shot and the velocity, and a shot's 'gradient' adds a
+    shot-dependent pattern scaled by its residual.  Device pointers are the
+    addresses of CPU tensors."""
+
+    def __init__(self, w):
+        self.nzz, self.nxx, self.nyy = w.nz + 2 * w.nb, w.nx + 2 * w.nb, w.ny + 2 * w.nb
+        self.nb, self.nt = w.nb, w.nt
+        shape = (self.nyy, self.nxx, self.nzz)
+        self.img, self.ill = np.zeros(shape, np.float32), np.zeros(shape, np.float32)
+        self.seeds = []
+
+    @staticmethod
+    def _view(ptr, n):
+        import ctypes
+        return np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ctypes.c_float)), shape=(n,))
+
+    def set_geometry(self, src, rec, first, count):
+        self.count = np.full(len(src), len(rec)) if count is None else np.asarray(count)
+
+    def shot_nrec(self, s):
+        return int(self.count[s])
+
+    def set_velocity(self, v):
+        self.v = np.asarray(v, np.float64)
+
+    def model_shots_dev(self, shots_, ptr):
+        off = 0
+        for s in shots_:
+            n = self.shot_nrec(s) * self.nt
+            i = np.arange(n)
+            seis = np.sin(1e-3 * (s + 1) * i) * self.v.mean() / 1000.0 + np.cos(self.v.ravel()[s] * 1e-3 + i)
+            self._view(ptr + 4 * off, n)[:] = seis.astype(np.float32)
+            off += n
+
+    def residual_dev(self, obs, cal, n, res):
+        r = self._view(obs, n) - self._view(cal, n)
+        self._view(res, n)[:] = r
+        return float(np.sum(r.astype(np.float64) ** 2))
+
+    def reset_accumulators(self):
+        self.img[:] = 0
+        self.ill[:] = 0
+
+    def set_shot_random_boundary(self, base_seed, **kw):
+        self.seeds.append(base_seed)
+
+    def gradient_shots_dev(self, shots_, ptr):
+        off = 0
+        for s in shots_:
+            n = self.shot_nrec(s) * self.nt
+            r = self._view(ptr + 4 * off, n).astype(np.float64)
+            pattern = np.cos(0.1 * (s + 1) * np.arange(self.img.size)).reshape(self.img.shape)
+            self.img += (pattern * r.sum()).astype(np.float32)
+            self.ill += np.float32(s + 1)
+            off += n
+
+    def get_accumulators_dev(self, img, ill):
+        self._view(img, self.img.size)[:] = self.img.ravel()
+        self._view(ill, self.ill.size)[:] = self.ill.ravel()
+
+    def set_accumulators_dev(self, img, ill):
+        self.img[:] = self._view(img, self.img.size).reshape(self.img.shape)
+        self.ill[:] = self._view(ill, self.ill.size).reshape(self.ill.shape)
+
+    def gradient_post(self, zmask):
+        nb = self.nb
+        g = self.img[nb:-nb, nb:-nb, nb:-nb] / self.ill[nb:-nb, nb:-nb, nb:-nb]
+        m = float(np.abs(g).max())
+        return (g / m).astype(np.float32), m
+
+    def get_accumulators(self):
+        return self.img.copy(), self.ill.copy()
+
+
+def _fwi_case():
+    from fwi3d_b200 import synth
+    w = synth.small_fwi(0, n=8, nt=16)
+    w.nb = 2
+    w.src = synth.surface_grid([10.0, 30.0, 50.0], [10.0, 40.0], 10.0)  # 6 shots
+    return w
+
+
+def _fwi_steps(world, rank):
+    """Misfit of the start model, one gradient, and the misfit of a second
+    model, through fwi.Fwi with world/rank."""
+    from fwi3d_b200 import fwi
+    w = _fwi_case()
+    prob = fwi.Fwi(w, fwi.FwiOptions(batch=2), world=world, rank=rank,
+                   contexts=(FakeContext(w), FakeContext(w)), device="cpu")
+    f0 = prob.misfit(w.start)
+    g, raw, ill, f1 = prob.gradient(w.start)
+    f2 = prob.misfit((w.start * 1.01).astype(np.float32))
+    return prob.mine, f0, f1, f2, g, raw, ill
+
+
+def _fwi_worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        q.put((rank, _fwi_steps(None, None)))  # world and rank from torch.distributed
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_fwi_misfit_and_gradient_equal_one_rank():
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_fwi_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = dict(q.get(timeout=180) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    one = _fwi_steps(1, 0)
+    assert sorted(out[0][0] + out[1][0]) == one[0] == list(range(6))
+    assert out[0][0] == [0, 2, 4] and out[1][0] == [1, 3, 5]
+    for r in (0, 1):
+        for k in (1, 2, 3):  # misfits: FP64 sums over every shot of every rank
+            assert abs(out[r][k] - one[k]) <= 1e-12 * abs(one[k]), (r, k)
+        assert out[r][1] == out[r][2]  # the gradient reuses the misfit of the same model
+        for k in (4, 5, 6):  # gradient, raw gradient, illumination: sums over shots
+            np.testing.assert_allclose(out[r][k], one[k], rtol=1e-5, atol=1e-6 * np.abs(one[k]).max())
+    np.testing.assert_array_equal(out[0][4], out[1][4])  # every rank takes the same step

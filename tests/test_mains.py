@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import oracle as orc
-from cases import TOL_SEIS, oracle_wavelet, rel_l2
+from cases import TOL_IMAGE, TOL_SEIS, oracle_wavelet, rel_l2
 from fwi3d_b200 import lib, synth
 
 pytestmark = pytest.mark.gpu
@@ -18,7 +18,7 @@ NZ, NX, NY, DH, NT, DT, FMAX = 24, 28, 26, 10.0, 150, 1e-3, 60.0
 ABC_LEN, ABC_F, RBC_LEN = 85.0, 0.02, 65.0  # nb = 9 and 7
 
 
-def write_setup(d: Path, vp, fixes=0, max_iteration=1):
+def write_setup(d: Path, vp, fixes=0, max_iteration=1, batch=1):
     d.mkdir(parents=True, exist_ok=True)
     for sub in ("data", "models", "seismic", "residuo"):
         (d / sub).mkdir(exist_ok=True)
@@ -59,6 +59,7 @@ mig_input_prefix = {prefix}
 mig_output_folder = {d}/seismic/
 b200_seed = 5
 b200_fixes = {fixes}
+b200_batch = {batch}
 """
     (d / "parameters.txt").write_text(text)
     return d / "parameters.txt", src, rec, prefix
@@ -100,7 +101,7 @@ def test_modeling_exe_matches_library_and_oracle(tmp_path, true_model):
         assert rel_l2(got, ref) < TOL_SEIS
 
 
-def test_migration_exe_matches_library(tmp_path, true_model):
+def test_migration_exe_matches_library_and_oracle(tmp_path, true_model):
     params, src, rec, prefix = write_setup(tmp_path, true_model)
     run("modeling.exe", params)
     out = run("migration.exe", params)
@@ -111,11 +112,34 @@ def test_migration_exe_matches_library(tmp_path, true_model):
     ctx = lib.Context(NZ, NX, NY, nb, DH, NT, DT, FMAX, lib.BOUNDARY_RBC)
     ctx.set_geometry(src, rec)
     ctx.set_velocity(true_model)
+    w = synth.Workload("t", NZ, NX, NY, DH, NT, DT, FMAX, nb, true_model, src, rec)
+    w64, _ = oracle_wavelet(ctx, w)
+    nzz, nxx = NZ + 2 * nb, NX + 2 * nb
+    flat = lambda p: orc.flat_index(orc.grid_index(float(p[2]), DH, nb), orc.grid_index(float(p[0]), DH, nb),
+                                    orc.grid_index(float(p[1]), DH, nb), nzz, nxx)
+    recf = np.array([flat(r) for r in rec], np.int64)
+    oimg = oill = None
     for s in range(2):
+        # shot s runs through the pad of seed b200_seed + s
         ctx.apply_random_boundary(kind=0, ratio=30.0, varVp=300.0, seed=5 + s)
         d = np.fromfile(tmp_path / "data" / f"{prefix}{s + 1}.bin", np.float32)
         ctx.rtm_shots([s], d)
+        vpp = ctx.get_padded_velocity()
+        _, P, Q = orc.forward(vpp, DH, DT, NT, ctx.tlag, w64, flat(src[s]), recf)
+        oimg, oill, _, _ = orc.backward(vpp, DH, DT, NT, ctx.tlag, recf, d.reshape(len(rec), NT), P, Q, mode=0,
+                                        image=oimg, illum=oill)
     assert np.array_equal(ctx.rtm_image().ravel(), img)
+    want = orc.rtm_post(oimg, oill, NZ, NX, NY, nb, DH)
+    assert rel_l2(img, want) < TOL_IMAGE, rel_l2(img, want)
+    # two shots per launch, each through its own pad: the same image up to the
+    # order of the sum over shots
+    params2, *_ = write_setup(tmp_path / "b2", true_model, batch=2)
+    for f in (tmp_path / "data").iterdir():
+        (tmp_path / "b2" / "data" / f.name).write_bytes(f.read_bytes())
+    run("migration.exe", params2)
+    img2 = np.fromfile(tmp_path / "b2" / "seismic" / f"RTM_section_{int(FMAX)}Hz_{NZ}x{NX}x{NY}_{int(DH)}m.bin",
+                       np.float32)
+    assert rel_l2(img2, img) < 1e-5
 
 
 @pytest.mark.parametrize("fixes,iters", [(0, 1), (1, 2)])
