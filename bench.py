@@ -5,12 +5,13 @@ Workload (default, the batched-RTM configuration): 201^3 model at 10 m, five
 layers plus -8 %/+12 % Gaussian anomalies, smoothed migration model, 50-cell
 random boundary (301^3 padded cells), nt = 2001 at 1 ms, Ricker 10 Hz peak
 (N = 2120 time steps), 64 shots on an 8 x 8 grid with clipped 121 x 121
-receiver patches.  One step = one shot's full RTM: new random boundary,
+receiver patches.  One step = one batch of B shots (--batch, default 4) in
+one launch per time step, each shot through its own new random boundary:
 forward propagation, then the fused pass (source rebuilt backwards + adjoint
-propagation + imaging), 3 padded cells x N steps of cell-updates.
+propagation + imaging), 3 x B padded cells x N steps of cell-updates.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload rtm|modeling]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B]
+                  [--impl ours|reference] [--workload rtm|modeling]
 
 Multi-GPU: one process per GPU (torchrun); shots are dealt round-robin to
 ranks (weak scaling) and the images are summed with one NCCL all-reduce at
@@ -175,12 +176,17 @@ def run_ours(args, ws, rank, local):
 
     w = workload(args.workload, args.nt)
     rtm = args.workload == "rtm"
+    B = args.batch if rtm else 1
     boundary = lib.BOUNDARY_RBC
-    ctx = lib.Context(w.nz, w.nx, w.ny, w.nb, w.dh, w.nt, w.dt, w.fmax, boundary, w.abc_factor, 1, 0)
+    ctx = lib.Context(w.nz, w.nx, w.ny, w.nb, w.dh, w.nt, w.dt, w.fmax, boundary, w.abc_factor, B, 0)
     stream = torch.cuda.Stream()
     ctx.set_stream(stream.cuda_stream)
     ctx.set_geometry(w.src, w.rec, w.rec_first, w.rec_count)
     ctx.set_velocity(w.start if w.start is not None else w.vp)
+    # shot s propagates through the random pad of seed 1000 + s, rebuilt for
+    # every batch inside the timed call (one velocity slot per batch slot)
+    rbc = dict(w.rbc)
+    ctx.set_shot_random_boundary(base_seed=1000, **rbc)
     if args.tiles:
         f, b = (int(x) for x in args.tiles.split(","))
         ctx.set_tiles(f, b)
@@ -189,36 +195,39 @@ def run_ours(args, ws, rank, local):
     nsrc = len(w.src)
     N = ctx.tlag + w.nt
     cells = ctx.nzz * ctx.nxx * ctx.nyy
-    updates_per_step = cells * N * (3 if rtm else 1)
+    updated = (ctx.nzz - 8) * (ctx.nxx - 8) * (ctx.nyy - 8)  # the 4-cell outer shell is never written
+    updates_per_step = cells * N * (3 if rtm else 1) * B
 
     from fwi3d_b200 import shots as shotlib
     total = args.warmup + args.steps
     mine = shotlib.partition(nsrc, ws, rank)
-    shots = [mine[k % len(mine)] for k in range(total)]
+    batches = [[mine[(k * B + j) % len(mine)] for j in range(B)] for k in range(total)]
     g = torch.Generator(device="cuda").manual_seed(1234 + rank)
     data = {}
     if rtm:
-        for s in set(shots):
-            data[s] = torch.randn(ctx.shot_nrec(s) * w.nt, generator=g, device="cuda", dtype=torch.float32)
+        for k, bt in enumerate(batches):
+            key = tuple(bt)
+            if key not in data:
+                n = sum(ctx.shot_nrec(s) for s in bt) * w.nt
+                data[key] = torch.randn(n, generator=g, device="cuda", dtype=torch.float32)
     seis_dev = None
     if not rtm:
         seis_dev = torch.empty(max(ctx.shot_nrec(s) for s in range(nsrc)) * w.nt, device="cuda")
-    rbc = dict(w.rbc)
     torch.cuda.synchronize()  # data come from the default stream; the library runs on `stream`
 
-    def step(s, timing):
-        ctx.apply_random_boundary(seed=1000 + s, **rbc)
+    def step(k, timing):
+        bt = batches[k]
         if rtm:
-            ctx.rtm_shots_dev([s], data[s].data_ptr())
+            ctx.rtm_shots_dev(bt, data[tuple(bt)].data_ptr())
         else:
-            ctx.model_shots_dev([s], seis_dev.data_ptr())
+            ctx.model_shots_dev(bt, seis_dev.data_ptr())
         f, b = ctx.last_timing()
         timing[0] += f
         timing[1] += b
 
     tw = [0.0, 0.0]
     for k in range(args.warmup):
-        step(shots[k], tw)
+        step(k, tw)
     torch.cuda.synchronize()
     barrier(ws)
     torch.cuda.synchronize()
@@ -233,7 +242,7 @@ def run_ours(args, ws, rank, local):
         with torch.cuda.stream(stream):
             e0.record(stream)
             for k in range(args.warmup, total):
-                step(shots[k], timing)
+                step(k, timing)
             if img_all is not None:
                 shotlib.reduce_context_accumulators(ctx, img_all, ill_all)
             e1.record(stream)
@@ -247,41 +256,52 @@ def run_ours(args, ws, rank, local):
     # roofline of the dominant kernel: the fused backward step (44 B per
     # cell-step) for RTM, the forward step (16 B per cell-update) for modeling
     peak, peak_kind = hbm_peak()
+    # per launch: B shots of the padded grid; frac_updated charges only the
+    # cells a launch writes (the outer 4-cell shell is read, never written)
     if rtm:
         kern_ms = timing[1] / args.steps / N
-        bytes_per_launch = 44.0 * cells
+        per_cell = 44.0
         name = "fd_backward_kernel"
     else:
         kern_ms = timing[0] / args.steps / N
-        bytes_per_launch = 16.0 * cells
+        per_cell = 16.0
         name = "fd_forward_kernel"
+    bytes_per_launch = per_cell * cells * B
     achieved = bytes_per_launch / (kern_ms / 1e3) / 1e9
+    achieved_upd = per_cell * updated * B / (kern_ms / 1e3) / 1e9
     traffic = None
     try:
         tr = json.loads(TRAFFIC.read_text())
         if name in tr:
-            traffic = float(tr[name]["bytes_per_cell"]) * cells
+            traffic = float(tr[name]["bytes_per_cell"]) * cells * B
     except Exception:
         pass
     fwd_ms = timing[0] / args.steps / N
+    fwd_upd = 16.0 * updated * B / (fwd_ms / 1e3) / 1e9
     roof = {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+            "achieved_updated": round(achieved_upd, 1), "frac_updated": round(achieved_upd / peak, 4),
             "traffic": traffic, "algorithmic_bytes": bytes_per_launch,
-            "launch_ms": round(kern_ms, 5),
-            "forward_kernel": {"achieved": round(16.0 * cells / (fwd_ms / 1e3) / 1e9, 1),
-                               "frac": round(16.0 * cells / (fwd_ms / 1e3) / 1e9 / peak, 4),
+            "algorithmic_bytes_updated": per_cell * updated * B,
+            "launch_ms": round(kern_ms, 5), "shots_per_launch": B,
+            "forward_kernel": {"achieved": round(16.0 * cells * B / (fwd_ms / 1e3) / 1e9, 1),
+                               "frac": round(16.0 * cells * B / (fwd_ms / 1e3) / 1e9 / peak, 4),
+                               "achieved_updated": round(fwd_upd, 1), "frac_updated": round(fwd_upd / peak, 4),
                                "launch_ms": round(fwd_ms, 5)}}
 
     # end to end through the public API with host buffers
     e2e = None
     if not args.no_e2e:
         host = {}
-        for s in set(shots[args.warmup:]):
-            n = (ctx.shot_nrec(s) * w.nt)
+        for bt in batches[args.warmup:]:
+            key = tuple(bt)
+            if key in host:
+                continue
+            n = sum(ctx.shot_nrec(s) for s in bt) * w.nt
             pin = torch.empty(n, dtype=torch.float32, pin_memory=True)
             if rtm:
-                pin.copy_(data[s].cpu())
-            host[s] = pin
+                pin.copy_(data[key].cpu())
+            host[key] = pin
         out = torch.empty(w.nz * w.nx * w.ny if rtm else max(ctx.shot_nrec(s) for s in range(nsrc)) * w.nt,
                           dtype=torch.float32, pin_memory=True)
         h2d = d2h = 0
@@ -290,15 +310,14 @@ def run_ours(args, ws, rank, local):
         with torch.cuda.stream(stream):
             e0.record(stream)
             for k in range(args.warmup, total):
-                s = shots[k]
-                ctx.apply_random_boundary(seed=1000 + s, **rbc)
+                bt = batches[k]
                 if rtm:
-                    ctx.rtm_shots([s], host[s].numpy())
+                    ctx.rtm_shots(bt, host[tuple(bt)].numpy())
                     ctx.rtm_image(out=out.numpy())  # straight into the pinned host buffer
-                    h2d += host[s].numel() * 4
+                    h2d += host[tuple(bt)].numel() * 4
                     d2h += out.numel() * 4
                 else:
-                    r = ctx.model_shots([s])[0]
+                    r = ctx.model_shots(bt)[0]
                     d2h += r.size * 4
             e1.record(stream)
         torch.cuda.synchronize()
@@ -325,13 +344,59 @@ def run_ours(args, ws, rank, local):
             "workload": (f"{w.name}: padded {ctx.nzz}x{ctx.nxx}x{ctx.nyy}, nt={w.nt}, N={N} steps; "
                          + ("one shot per step: random boundary + forward + fused backward (3 cell-updates "
                             "per padded cell per step)" if rtm else "one shot per step: forward modeling")),
-            "shots": nsrc, "l2": l2_note,
+            "shots": nsrc, "shots_per_step": B, "shots_per_launch": B, "l2": l2_note,
             "tiles": ctx.tiles(), "parallelism": f"shots/{ws}"},
         "roofline": roof,
         "e2e": e2e,
         "gpu_launches": int(launches),
     }
     return line, clocks.summary()
+
+
+def secondary_modeling(steps=5, warmup=2):
+    """The plain-modeling configuration (101^3 model + 50-cell random pad,
+    201^3 padded cells, nt = 1001, N = 1120, one shot, 51 x 51 receivers),
+    measured in the same run: device time per shot with CUDA events on the
+    library's stream, and the forward kernel's HBM fraction.  Its working set
+    (3 fields x 32.5 MB) fits in the 126 MB L2."""
+    import torch
+    from fwi3d_b200 import lib
+    w = workload("modeling")
+    ctx = lib.Context(w.nz, w.nx, w.ny, w.nb, w.dh, w.nt, w.dt, w.fmax, lib.BOUNDARY_RBC, w.abc_factor, 1, 0)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_geometry(w.src, w.rec)
+    ctx.set_velocity(w.vp)
+    ctx.set_shot_random_boundary(base_seed=1, **w.rbc)
+    ctx.autotune()
+    seis = torch.empty(len(w.rec) * w.nt, device="cuda")
+    torch.cuda.synchronize()
+    for _ in range(warmup):
+        ctx.model_shots_dev([0], seis.data_ptr())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fwd = 0.0
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(steps):
+            ctx.model_shots_dev([0], seis.data_ptr())
+            fwd += ctx.last_timing()[0]
+        e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    N = ctx.tlag + w.nt
+    cells = ctx.nzz * ctx.nxx * ctx.nyy
+    updated = (ctx.nzz - 8) * (ctx.nxx - 8) * (ctx.nyy - 8)
+    peak, _ = hbm_peak()
+    kern = fwd / steps / N
+    ctx.close()
+    return {"workload": f"{w.name}: padded {cells ** (1 / 3):.0f}^3, nt={w.nt}, N={N}, one shot, "
+                        f"{len(w.rec)} receivers; random pad",
+            "value": round(cells * N / (ms / 1e3) / 1e6, 1), "unit": "Mcell-updates/s",
+            "ms_per_step": round(ms, 3), "steps": steps, "warmup": warmup,
+            "forward_kernel": {"launch_ms": round(kern, 5),
+                               "frac": round(16.0 * cells / (kern / 1e3) / 1e9 / peak, 4),
+                               "frac_updated": round(16.0 * updated / (kern / 1e3) / 1e9 / peak, 4)},
+            "l2": "working set 3 fields x 32.5 MB, below the 126 MB L2"}
 
 
 def run_reference(args, ws, rank, local):
@@ -405,6 +470,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["rtm", "modeling"], default="rtm")
+    ap.add_argument("--batch", type=int, default=4, help="shots per launch (RTM)")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the plain-modeling (101^3 + 50-cell pad) secondary measurement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
     ap.add_argument("--tiles", default="", help="fixed forward,backward tile indices instead of autotuning")
@@ -421,6 +489,8 @@ def main():
             line["clocks"] = clocks
         if args.impl == "ours" and ws == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(workload(args.workload))
+        if args.impl == "ours" and ws == 1 and args.workload == "rtm" and not args.no_secondary:
+            line["secondary"] = secondary_modeling()
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist

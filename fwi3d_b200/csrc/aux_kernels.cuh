@@ -103,7 +103,7 @@ __global__ void start_source_kernel(float *__restrict__ A, long long vol, int ld
 // ---------------------------------------------------------------------------
 // Adjoint injection: Pr[cell] += idh3 * d(receiver) for every receiver on the
 // cell, time-reversed (inject_seismogram / inject_residuo,
-// src/migration/migration.cu:166-179, src/inversion/inversion.cu:476-489).
+// src/migration/migration.cu:119-132, src/inversion/inversion.cu:385-398).
 // Receivers sharing a cell are added one after another in receiver order,
 // which keeps the sum deterministic where the reference uses atomicAdd.
 // ---------------------------------------------------------------------------
@@ -141,7 +141,7 @@ __global__ void transpose_kernel(const float *__restrict__ in, long long rows, l
 // ---------------------------------------------------------------------------
 // RTM image: crop, divide by illumination, -d2/dz2 * idh2 with the first and
 // last depth sample 0 (Migration::export_seismic,
-// src/migration/migration.cu:137-164), FP32 like the reference.
+// src/migration/migration.cu:90-117), FP32 like the reference.
 // ---------------------------------------------------------------------------
 // Image or gradient over illumination.  A cell the source field never
 // reached has illumination 0 and no image either; the reference's 0/0 there
@@ -172,7 +172,7 @@ __global__ void rtm_image_kernel(const float *__restrict__ img, const float *__r
 }
 
 // Gradient post-processing, first pass: crop, divide, -d2/dz2 below the mask
-// and the running max |g| (src/inversion/inversion.cu:233-256).  max|g| of
+// and the running max |g| (src/inversion/inversion.cu:142-165).  max|g| of
 // non-negative floats is taken with an integer atomicMax on their bits, which
 // is exact and order independent.
 __global__ void grad_post_kernel(const float *__restrict__ g, const float *__restrict__ ill, int nz,
@@ -201,7 +201,7 @@ __global__ void grad_post_kernel(const float *__restrict__ g, const float *__res
     if ((threadIdx.x & 31) == 0) atomicMax(gmax_bits, __float_as_uint(lmax));
 }
 
-// Second pass: g *= 1/gmax (src/inversion/inversion.cu:258-260).
+// Second pass: g *= 1/gmax (src/inversion/inversion.cu:167-169).
 __global__ void scale_by_inverse_kernel(float *__restrict__ g, long long n,
                                         const unsigned int *__restrict__ gmax_bits)
 {
@@ -231,7 +231,7 @@ __device__ __forceinline__ double block_sum(double v)
 }
 
 // res = obs - cal (FP32, as the reference stores it) and sum(res^2) in FP64
-// (src/inversion/inversion.cu:285-289).
+// (src/inversion/inversion.cu:194-198).
 template <int NT>
 __global__ void __launch_bounds__(NT)
     residual_partial_kernel(const float *__restrict__ obs, const float *__restrict__ cal,

@@ -936,7 +936,7 @@ double residual_impl(fwi_ctx *c, const float *d_obs, const float *d_cal, long lo
 }
 
 // Host Poisson-disk sampling (Bridson's method, as poissonDiskSampling of
-// src/admin/admin.cpp:138-241: up to 30 candidates in the shell [r, 2r] around
+// src/admin/admin.cpp:105-207: up to 30 candidates in the shell [r, 2r] around
 // a random active point), seeded and deterministic.  Only points outside the
 // inner box `keep_out` are kept by the random boundary (modeling.cu:571-577),
 // so candidates inside it are rejected outright and the sampling covers the
@@ -1104,7 +1104,7 @@ void check_rbc(const fwi_rbc *rbc)
 bool wants_blobs(const fwi_rbc *rbc) { return rbc->kind == 0 && rbc->ratio > 0 && rbc->varVp > 0; }
 
 // Clamp of the pad: kind 0 keeps [vmin - varVp, vmax + varVp] like the
-// reference's blob kernel (src/modeling/modeling.cu:611-612); both kinds stay
+// reference's blob kernel (src/modeling/modeling.cu:612-613); both kinds stay
 // at or below cfl_cap times the leapfrog stability velocity.
 void rbc_bounds(const fwi_ctx *c, const fwi_rbc *rbc, float &vlo, float &vhi)
 {

@@ -25,7 +25,7 @@ int copy_out(const std::string &v, char *out, int cap)
 
 extern "C" {
 
-// catch_parameter (src/admin/admin.cpp:86-121): the first line that does not
+// catch_parameter (src/admin/admin.cpp:53-88): the first line that does not
 // start with '#' or ' ' and starts with `key` (a prefix match) gives the
 // value: the text from two characters after the first '=' up to a '#', with
 // every space removed.  A missing key gives an empty value (FWI_OK), an
@@ -53,7 +53,7 @@ int fwi_catch_parameter(const char *file, const char *key, char *value, int cap)
 }
 
 // SPS/RPS point file (src/geometry/geometry.cpp:3-47 with import_text_file,
-// src/admin/admin.cpp:72-84): one "x,y,z" line per point in metres, lines
+// src/admin/admin.cpp:39-51): one "x,y,z" line per point in metres, lines
 // starting with '#' skipped.  With x == NULL only the count is returned.
 int fwi_read_points(const char *file, float *x, float *y, float *z, int cap, int *n)
 {
@@ -85,7 +85,7 @@ int fwi_read_points(const char *file, float *x, float *y, float *z, int cap, int
     return FWI_OK;
 }
 
-// import_binary_float / export_binary_float (src/admin/admin.cpp:46-70).
+// import_binary_float / export_binary_float (src/admin/admin.cpp:13-37).
 int fwi_read_binary(const char *file, float *buf, int64_t n)
 {
     if (!file || (!buf && n > 0) || n < 0) return FWI_ERR_ARG;

@@ -9,8 +9,8 @@
 //                       Ps    <- dt^2 v^2 lap(Psold) + 2 Psold - Ps  (source rebuilt)
 //                       Prold <- dt^2 v^2 lap(Pr) + 2 Pr - Prold      (adjoint)
 //                       illum += Ps^2 ; image += Ps Pr  or  the gradient term
-//                       (reference: cross_correlation, src/migration/migration.cu:181-248;
-//                        build_gradient, src/inversion/inversion.cu:491-558)
+//                       (reference: cross_correlation, src/migration/migration.cu:134-202;
+//                        build_gradient, src/inversion/inversion.cu:400-468)
 //
 // Data layout in HBM: every field of one shot is a pitched [nyy][nxx][ldz] FP32
 // array (z fastest, ldz = nzz rounded up to 8); the shots of a batch follow

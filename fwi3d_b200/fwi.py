@@ -13,7 +13,7 @@ random boundary per shot) and makes the step search measured:
   - every candidate step's misfit is computed, never predicted;
   - while the misfit still falls at the largest step tried, the step doubles
     (the reference stops at its two trials and extrapolates the parabola
-    without bound, inversion.cu:331-347);
+    without bound, inversion.cu:291-313);
   - the parabola's vertex through the best step and its neighbours is then
     measured too, and the best measured candidate is taken;
   - every step stays within STEP_BOUND x 0.05 dm and the MAX_DV trust region,
@@ -43,7 +43,7 @@ from .synth import Workload
 
 # Largest step as a multiple of the 0.05 dm trial step (inversion.exe uses the
 # same bound): the reference's parabola vertex is unbounded and can leave the
-# physical range (inversion.cu:331-347).
+# physical range (inversion.cu:309-312).
 STEP_BOUND = 8.0
 # Trust region of the plain update: no cell's velocity changes by more than
 # this fraction in one iteration.
@@ -76,7 +76,7 @@ def model_key(v) -> bytes:
 
 def parabola_vertex(a, r):
     """Vertex of the parabola through (a_i, r_i), i = 0..2 (the reference's
-    formula, inversion.cu:331-347); None when it is not a minimum."""
+    formula, inversion.cu:309-312); None when it is not a minimum."""
     num = (a[1] ** 2 - a[2] ** 2) * r[0] + (a[2] ** 2 - a[0] ** 2) * r[1] + (a[0] ** 2 - a[1] ** 2) * r[2]
     den = (a[1] - a[2]) * r[0] + (a[2] - a[0]) * r[1] + (a[0] - a[1]) * r[2]
     # positive second divided difference: a minimum

@@ -1,6 +1,6 @@
 // inversion.exe parameters.txt -- drop-in for src/inversion_main.cpp.
 //
-// The reference's FWI loop (src/inversion/inversion.cu:94-474):
+// The reference's FWI loop (src/inversion_main.cpp:13-22, src/inversion/inversion.cu:115-383):
 //   compute_gradient   per shot: observed data, modelled data in the Cerjan
 //                      grid, residual obs-cal and its squared norm, then (while
 //                      iteration <= max_iteration) the gradient through a fresh
@@ -64,7 +64,7 @@ struct Inversion {
                        "fwi_residual");
             sum += sq;
             if (grad) {
-                // update_RBC (inversion.cu:295-307): the ABC model, re-padded, new random pad
+                // update_RBC (inversion.cu:204-216): the ABC model, re-padded, new random pad
                 fwh::check(fwi_set_velocity(rbc, v_abc.data()), rbc, "fwi_set_velocity");
                 fwh::check(fwi_apply_random_boundary(rbc, &rbc_recipe, (uint64_t)(seed + s + 7919 * iteration)),
                            rbc, "random boundary");
@@ -93,7 +93,7 @@ struct Inversion {
         fwh::check(fwi_set_velocity(abc, v_abc.data()), abc, "fwi_set_velocity");
     }
 
-    // linesearch (inversion.cu:406-438): misfit of the trial model m - alpha g.
+    // linesearch (inversion.cu:315-347): misfit of the trial model m - alpha g.
     float linesearch(float alpha)
     {
         std::vector<float> v(npts);
@@ -190,7 +190,7 @@ int main(int argc, char **argv)
         fwh::Clock clock;
         for (;;) {
             I.compute_gradient();
-            ++I.iteration;  // check_convergence (inversion.cu:371-380)
+            ++I.iteration;  // check_convergence (inversion.cu:280-289)
             std::cout << "Residuo " << I.residuo.size() - 1 << ": " << I.residuo.back() << "\n";
             if (I.iteration > I.max_iteration) break;
             I.optimization_and_update();

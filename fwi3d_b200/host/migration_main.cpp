@@ -1,10 +1,10 @@
 // migration.exe parameters.txt -- drop-in for src/migration_main.cpp.
 //
-// Reads the same keys (src/migration/migration.cu:50-83): a random boundary of
+// Reads the same keys (src/migration/migration.cu:9-23): a random boundary of
 // int(mig_rbc_length/dh)+1 cells with mig_rbc_ratio / mig_rbc_varVp, the shot
 // data {mig_input_folder}{mig_input_prefix}{s+1}.bin, and writes
 // {mig_output_folder}RTM_section_{int(fmax)}Hz_{nz}x{nx}x{ny}_{int(dh)}m.bin
-// (export_seismic, migration.cu:137-164).
+// (export_seismic, migration.cu:90-117).
 // Optional keys: b200_batch (shots per launch), b200_seed (random-boundary
 // seed of shot s is b200_seed + s; the reference seeds from the clock),
 // b200_fixes (default 1: remove the source while rebuilding the forward

@@ -16,7 +16,7 @@ namespace fwh {
 
 // A failing ABI call becomes an exception with the library's message; main()
 // prints it in red and exits 1, like the reference's uncaught
-// std::invalid_argument (src/admin/admin.cpp:50-51).
+// std::invalid_argument (src/admin/admin.cpp:17-18).
 inline void check(int st, fwi_ctx *ctx, const char *what)
 {
     if (st == FWI_OK) return;
@@ -29,7 +29,7 @@ inline void check(int st, fwi_ctx *ctx, const char *what)
     throw std::runtime_error(msg);
 }
 
-// catch_parameter(key, file) (src/admin/admin.cpp:86-121).
+// catch_parameter(key, file) (src/admin/admin.cpp:53-88).
 inline std::string param(const std::string &file, const std::string &key)
 {
     char buf[4096];
@@ -109,7 +109,7 @@ inline Model read_model(const std::string &pf)
     return m;
 }
 
-// Pad width: int(length / dh) + 1 (src/modeling/modeling.cu:90, migration.cu:60).
+// Pad width: int(length / dh) + 1 (src/modeling/modeling.cu:90, migration.cu:13).
 inline int pad_cells(float length, float dh) { return (int)(length / dh) + 1; }
 
 inline fwi_ctx *make_context(const Model &m, int nb, int boundary, float abc_factor, int batch, int flags)

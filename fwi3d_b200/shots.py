@@ -2,7 +2,7 @@
 ranks, one sum of the images (or gradients) and of the FP64 misfit at the end.
 
 The reference is single-GPU (no NCCL or MPI anywhere); its shots are
-independent (src/migration_main.cpp:15-21, src/inversion/inversion.cu:214-229),
+independent (src/migration_main.cpp:13-19, src/inversion/inversion.cu:123-138),
 so the only exchange is the final sum.  Collectives go through
 torch.distributed (NCCL between GPUs, gloo in the CPU tests).
 """

@@ -12,7 +12,7 @@
  * Conventions
  *   - Volumes are float32, z fastest, then x, then y (Fortran [nz, nx, ny]),
  *     as read by src/modeling/modeling.cu:160-162 and written by
- *     src/migration/migration.cu:162-163.
+ *     src/migration/migration.cu:115-116.
  *   - Seismograms are float32 Fortran [nt, nrec] (sample t of receiver r at
  *     t + r*nt), as written by src/modeling/modeling.cu:302-307.
  *   - Host buffers are owned by the caller; device buffers by the library.
@@ -50,16 +50,16 @@ extern "C" {
 
 /* behaviour flags (fwi_params.flags) */
 #define FWI_FLAG_GRAD_DY 0x1        /* include d2/dy2 in the gradient (reference omits it,
-                                       src/inversion/inversion.cu:557) */
+                                       src/inversion/inversion.cu:466) */
 #define FWI_FLAG_SUBTRACT_SOURCE 0x2 /* remove the source while rebuilding the forward field
-                                       backwards (reference does not, migration.cu:242) */
+                                       backwards (reference does not, migration.cu:195) */
 
 typedef struct fwi_ctx fwi_ctx;
 
 /* Grid: the unpadded model plus the pad width.
  * Replaces Modeling::set_main_parameters / set_properties
  * (src/modeling/modeling.cu:17-34, 142-179) and Migration/Inversion's
- * nb = int(length/dh)+1 (src/migration/migration.cu:60, inversion.cu:148,175). */
+ * nb = int(length/dh)+1 (src/migration/migration.cu:13, inversion.cu:57, 84). */
 typedef struct {
     int nz, nx, ny;   /* z_samples, x_samples, y_samples */
     int nb;           /* pad cells on every side */
@@ -153,14 +153,14 @@ int fwi_model_shots_dev(fwi_ctx *ctx, const int *shots, int nshots, float *d_sei
  * accumulate image += Ps*Pr, illum += Ps^2.  data holds each shot's
  * [nt, nrec_s] seismogram one after another.  Replaces
  * Migration::forward_propagation + backward_propagation
- * (src/migration/migration.cu:96-128, 166-248). */
+ * (src/migration/migration.cu:49-81, 119-202). */
 int fwi_rtm_shots(fwi_ctx *ctx, const int *shots, int nshots, const float *data);
 int fwi_rtm_shots_dev(fwi_ctx *ctx, const int *shots, int nshots, const float *d_data);
 /* Zero the padded image / gradient and illumination accumulators. */
 int fwi_reset_accumulators(fwi_ctx *ctx);
 /* Zero only the image / gradient accumulator and keep the illumination: the
- * reference zeroes its gradient for every gradient (inversion.cu:210) but never
- * its illumination (d_sumPs_rbc, inversion.cu:142). */
+ * reference zeroes its gradient for every gradient (inversion.cu:119) but never
+ * its illumination (d_sumPs_rbc, inversion.cu:51, 145). */
 int fwi_zero_image(fwi_ctx *ctx);
 /* Raw padded accumulators [nzz,nxx,nyy] (either pointer may be NULL). */
 int fwi_get_accumulators(fwi_ctx *ctx, float *image_padded, float *illum_padded);
@@ -171,21 +171,21 @@ int fwi_get_accumulators_dev(fwi_ctx *ctx, float *d_image_padded, float *d_illum
  * such a sum, or to resume from a saved image). */
 int fwi_set_accumulators_dev(fwi_ctx *ctx, const float *d_image_padded, const float *d_illum_padded);
 /* Final image [nz,nx,ny]: crop, divide by illumination, -d2/dz2
- * (replaces Migration::export_seismic, src/migration/migration.cu:137-164). */
+ * (replaces Migration::export_seismic, src/migration/migration.cu:90-117). */
 int fwi_rtm_image(fwi_ctx *ctx, float *image);
 
 /* ---- inversion --------------------------------------------------------- */
 /* Same fused pass with the gradient imaging condition
- * grad += dt*Pr*(d2x+d2z[+d2y])Ps*v^2 (src/inversion/inversion.cu:491-558);
+ * grad += dt*Pr*(d2x+d2z[+d2y])Ps*v^2 (src/inversion/inversion.cu:400-468);
  * residual holds each shot's [nt, nrec_s] obs-cal one after another. */
 int fwi_gradient_shots(fwi_ctx *ctx, const int *shots, int nshots, const float *residual);
 int fwi_gradient_shots_dev(fwi_ctx *ctx, const int *shots, int nshots, const float *d_residual);
 /* Gradient post-processing [nz,nx,ny]: crop, divide by illumination, -d2/dz2
- * below int(zmask/dh), divide by max|g| (src/inversion/inversion.cu:233-260).
+ * below int(zmask/dh), divide by max|g| (src/inversion/inversion.cu:142-169).
  * gmax receives max|g| before normalisation (may be NULL). */
 int fwi_gradient_post(fwi_ctx *ctx, float zmask, float *grad, float *gmax);
 /* Residual obs - cal and its sum of squares, accumulated in FP64 on the GPU
- * (replaces the FP32 host loop of src/inversion/inversion.cu:281-292).
+ * (replaces the FP32 host loop of src/inversion/inversion.cu:190-201).
  * res may be NULL. */
 int fwi_residual(fwi_ctx *ctx, const float *obs, const float *cal, int64_t n, float *res,
                  double *sum_sq);
@@ -237,14 +237,14 @@ int fwi_prepare_rtm_input(const float *seis, float *out, int nt, int nrec, const
                           float sx, float sy, float velocity, float time_delay, float dt, float gstd);
 
 /* ---- reference file formats (host only, no device needed) --------------- */
-/* catch_parameter (src/admin/admin.cpp:86-121): value of the first line that
+/* catch_parameter (src/admin/admin.cpp:53-88): value of the first line that
  * starts with `key` and not with '#' or ' ' -- a prefix match -- taken from two
  * characters after '=' up to '#', spaces removed.  Missing key: empty value. */
 int fwi_catch_parameter(const char *parameters_file, const char *key, char *value, int cap);
 /* SPS/RPS "x,y,z" lines in metres, '#' lines skipped (src/geometry/geometry.cpp:
  * 3-47).  x == NULL returns only the count in *n. */
 int fwi_read_points(const char *file, float *x, float *y, float *z, int cap, int *n);
-/* Raw float32 files (import/export_binary_float, src/admin/admin.cpp:46-70). */
+/* Raw float32 files (import/export_binary_float, src/admin/admin.cpp:13-37). */
 int fwi_read_binary(const char *file, float *buf, int64_t n);
 int fwi_write_binary(const char *file, const float *buf, int64_t n);
 

@@ -22,10 +22,13 @@
  *     (src/modeling/modeling.cu:391); the oracle leaves it at 0.
  *
  * Parity pins: tests/golden/ holds outputs of the reference's own CUDA kernels
- * (built from source by oracle/Makefile into oracle/_ref and run on a B200),
- * and tests/test_oracle.py checks this file against them and against analytic
- * known answers (plane-wave dispersion, constant-velocity Green's function,
- * adjoint dot-product identity).
+ * (built from source by oracle/Makefile into oracle/_ref and run on a B200);
+ * tests/test_golden.py checks this file against them, tests/test_reference_build.py
+ * and tests/test_fullsize_parity.py against the live reference build, and
+ * tests/test_known_answers.py against analytic known answers (eighth-order
+ * stencil symbol, constant-velocity Green's function, finite-difference
+ * gradient) and the dot-product identity of the imaging operator with
+ * orc_image_adjoint.
  *
  * Build: oracle/Makefile -> oracle/liboracle.so (gcc -O3 -fopenmp).
  */
@@ -270,8 +273,8 @@ void orc_forward(int nzz, int nxx, int nyy, double dh, double dt, int nt, int tl
 }
 
 /* ------------------------------------------------------------------------ */
-/* Adjoint source: src/migration/migration.cu:166-179 and                     */
-/* src/inversion/inversion.cu:476-489 -- time-reversed data added at the     */
+/* Adjoint source: src/migration/migration.cu:119-132 and                     */
+/* src/inversion/inversion.cu:385-398 -- time-reversed data added at the     */
 /* receiver cells, scaled by idh3, for t < nt.                               */
 /* ------------------------------------------------------------------------ */
 static void inject_reversed(double *Pr, int nt, int t, int nrec, const long *rec,
@@ -283,16 +286,16 @@ static void inject_reversed(double *Pr, int nt, int t, int nrec, const long *rec
 
 /* ------------------------------------------------------------------------ */
 /* Back-propagation of one shot through a non-damping (random) boundary.     */
-/*   mode 0 (RTM)      src/migration/migration.cu:108-128 + 181-248          */
+/*   mode 0 (RTM)      src/migration/migration.cu:61-81 + 134-202            */
 /*       Ps    <- dt^2 v^2 lap(Psold) + 2 Psold - Ps     (source rebuilt)    */
 /*       Prold <- dt^2 v^2 lap(Pr) + 2 Pr - Prold        (adjoint field)     */
 /*       illum += Ps^2 ; image += Ps Pr                                       */
-/*   mode 1 (gradient) src/inversion/inversion.cu:326-344 + 491-558          */
+/*   mode 1 (gradient) src/inversion/inversion.cu:235-253 + 400-468          */
 /*       same two updates; illum += Ps^2 ;                                   */
 /*       image += dt Pr (d2x Psold + d2z Psold [+ d2y Psold]) v^2            */
-/*       The reference omits d2y (inversion.cu:557); with_dy=1 restores it.  */
+/*       The reference omits d2y (inversion.cu:466); with_dy=1 restores it.  */
 /* subtract_src = 1 removes the source term while rebuilding Ps (the        */
-/* reference does not, migration.cu:242); w, src and tlag give that term.    */
+/* reference does not, migration.cu:195); w, src and tlag give that term.    */
 /* Ps, Psold in: the forward pair (u^N, u^{N-1}); out: rebuilt fields.       */
 /* ------------------------------------------------------------------------ */
 void orc_backward(int nzz, int nxx, int nyy, double dh, double dt, int nt, int tlag,
@@ -347,7 +350,87 @@ void orc_backward(int nzz, int nxx, int nyy, double dh, double dt, int nt, int t
 }
 
 /* ------------------------------------------------------------------------ */
-/* RTM image post-processing: src/migration/migration.cu:137-164.            */
+/* Adjoint of the imaging operator of orc_backward (mode 0) for fixed source  */
+/* fields: the image is sum_t S_t . u_t, where S_t is the rebuilt source     */
+/* field of back-propagation step t and u_t the adjoint field after the      */
+/* injection of step t, with                                                  */
+/*     u_{t+1} = (2 + V L) u_t - u_{t-1} + J_{t+1} d,   V = dt^2 v^2,         */
+/* L the interior Laplacian (zero outer shell) and J_t the injection of      */
+/* idh3 d[r, nt-1-t] at the receiver cells (src/migration/migration.cu:       */
+/* 61-81, 119-202).  Its adjoint runs                                         */
+/*     lambda_t = (2 + L V) lambda_{t+1} - lambda_{t+2} + S_t . m            */
+/* from t = N-1 down to 0 and reads data[r, nt-1-t] = idh3 lambda_t(rec r):  */
+/* Born modelling of the model m scattering the source field.  Ps0, Psold0   */
+/* are the forward pair handed to orc_backward; subtract_src, w and src as   */
+/* there.  For the dot-product test <image(d), m> = <d, adjoint(m)>; keeps   */
+/* all N source fields in memory (small grids only).                          */
+/* ------------------------------------------------------------------------ */
+int orc_image_adjoint(int nzz, int nxx, int nyy, double dh, double dt, int nt, int tlag,
+                      const double *vp, int nrec, const long *rec, int subtract_src, const double *w,
+                      long src, const double *Ps0, const double *Psold0, const double *m, double *data)
+{
+    const size_t sz = 1, sx = (size_t)nzz, sy = (size_t)nzz * nxx;
+    const size_t vol = (size_t)nzz * nxx * nyy;
+    const double idh2 = 1.0 / (dh * dh), idh3 = 1.0 / (dh * dh * dh), dt2 = dt * dt;
+    const int N = nt + tlag;
+    double *S = (double *)calloc((size_t)N * vol, sizeof(double));
+    double *ps = (double *)malloc(vol * sizeof(double));
+    double *pso = (double *)malloc(vol * sizeof(double));
+    double *l0 = (double *)calloc(vol, sizeof(double));  /* lambda_{t+1} */
+    double *l1 = (double *)calloc(vol, sizeof(double));  /* lambda_{t+2} */
+    double *vl = (double *)calloc(vol, sizeof(double));  /* V lambda_{t+1} */
+    if (!S || !ps || !pso || !l0 || !l1 || !vl) {
+        free(S); free(ps); free(pso); free(l0); free(l1); free(vl);
+        return 1;
+    }
+    memcpy(ps, Ps0, vol * sizeof(double));
+    memcpy(pso, Psold0, vol * sizeof(double));
+    /* the source fields exactly as orc_backward rebuilds them */
+    for (int t = 0; t < N; ++t) {
+        const double scorr = (subtract_src && (N - t) < nt) ? idh3 * w[N - t] : 0.0;
+        double *St = S + (size_t)t * vol;
+#pragma omp parallel for
+        for (int k = 4; k < nyy - 4; ++k)
+            for (int j = 4; j < nxx - 4; ++j)
+                for (int i = 4; i < nzz - 4; ++i) {
+                    size_t c = i + j * sx + k * sy;
+                    double lap = (d2_axis(pso, c, sx) + d2_axis(pso, c, sy) + d2_axis(pso, c, sz)) * idh2;
+                    double psn = dt2 * vp[c] * vp[c] * lap + 2.0 * pso[c] - ps[c];
+                    if ((long)c == src) psn += scorr;
+                    St[c] = psn;
+                }
+        for (size_t c = 0; c < vol; ++c) ps[c] = St[c];
+        double *tmp = ps; ps = pso; pso = tmp;
+    }
+    memset(data, 0, (size_t)nrec * nt * sizeof(double));
+    for (int t = N - 1; t >= 0; --t) {
+        const double *St = S + (size_t)t * vol;
+#pragma omp parallel for
+        for (int k = 4; k < nyy - 4; ++k)
+            for (int j = 4; j < nxx - 4; ++j)
+                for (int i = 4; i < nzz - 4; ++i) {
+                    size_t c = i + j * sx + k * sy;
+                    vl[c] = dt2 * vp[c] * vp[c] * l0[c];
+                }
+        /* lambda_t overwrites lambda_{t+2} */
+#pragma omp parallel for
+        for (int k = 4; k < nyy - 4; ++k)
+            for (int j = 4; j < nxx - 4; ++j)
+                for (int i = 4; i < nzz - 4; ++i) {
+                    size_t c = i + j * sx + k * sy;
+                    double lap = (d2_axis(vl, c, sx) + d2_axis(vl, c, sy) + d2_axis(vl, c, sz)) * idh2;
+                    l1[c] = 2.0 * l0[c] + lap - l1[c] + St[c] * m[c];
+                }
+        if (t < nt)
+            for (int r = 0; r < nrec; ++r) data[(nt - 1 - t) + (size_t)r * nt] += idh3 * l1[rec[r]];
+        double *tmp = l0; l0 = l1; l1 = tmp;
+    }
+    free(S); free(ps); free(pso); free(l0); free(l1); free(vl);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* RTM image post-processing: src/migration/migration.cu:90-117.             */
 /* Crop image and illumination, divide, then -d2/dz2 scaled by idh2 with the  */
 /* first and last depth sample set to 0.                                     */
 /* ------------------------------------------------------------------------ */
@@ -373,7 +456,7 @@ void orc_rtm_post(const double *image_pad, const double *illum_pad, int nz, int 
 }
 
 /* ------------------------------------------------------------------------ */
-/* FWI gradient post-processing: src/inversion/inversion.cu:233-260.         */
+/* FWI gradient post-processing: src/inversion/inversion.cu:142-169.         */
 /* Crop, divide by illumination, -d2/dz2 below the depth mask               */
 /* (i > int(zmask/dh) and i < nz-1), normalise by max |g|.  Returns max|g|.  */
 /* ------------------------------------------------------------------------ */
@@ -403,7 +486,7 @@ double orc_gradient_post(const double *grad_pad, const double *illum_pad, int nz
 }
 
 /* ------------------------------------------------------------------------ */
-/* Residual and L2 misfit: src/inversion/inversion.cu:281-292.               */
+/* Residual and L2 misfit: src/inversion/inversion.cu:190-201.               */
 /* res = obs - cal ; returns sum(res^2) (the reference sums in FP32).        */
 /* ------------------------------------------------------------------------ */
 double orc_residual(const double *obs, const double *cal, long n, double *res)
@@ -430,7 +513,7 @@ double orc_residual_f32(const float *obs, const float *cal, long n)
 }
 
 /* ------------------------------------------------------------------------ */
-/* Parabolic line search: src/inversion/inversion.cu:382-404.                */
+/* Parabolic line search: src/inversion/inversion.cu:291-313.                */
 /* Fit f(a) through (a0,f0),(a1,f1),(a2,f2) and return the vertex.           */
 /* ------------------------------------------------------------------------ */
 double orc_parabola_step(double a0, double a1, double a2, double f0, double f1, double f2)
@@ -440,7 +523,7 @@ double orc_parabola_step(double a0, double a1, double a2, double f0, double f1, 
     return 0.5 * num / den;
 }
 
-/* Trial / updated velocity in slowness-squared: inversion.cu:406-412, 440-447.
+/* Trial / updated velocity in slowness-squared: inversion.cu:315-321, 349-356.
  * m = 1/v^2 ; v' = 1/sqrt(m - alpha g). */
 void orc_model_step(const double *m, const double *g, long n, double alpha, double *v_out)
 {

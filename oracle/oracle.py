@@ -59,6 +59,8 @@ def load():
             "orc_model_step": (None, [_dp, _dp, _l, _d, _dp]),
             "orc_step": (None, [_i, _i, _i, _d, _d, _dp, _dp, _dp]),
             "orc_laplacian": (None, [_i, _i, _i, _d, _dp, _dp]),
+            "orc_image_adjoint": (_i, [_i, _i, _i, _d, _d, _i, _i, _dp, _i, _lp, _i, _dp, _l, _dp, _dp, _dp,
+                                       _dp]),
         }
         for k, (r, a) in sig.items():
             f = getattr(lib, k)
@@ -150,6 +152,23 @@ def backward(vpp, dh, dt, nt, tlag, rec, data, Ps, Psold, mode=0, with_dy=False,
                         _p(data), mode, int(with_dy), int(subtract_src), _p(w), int(src),
                         _p(Ps), _p(Psold), _p(image), _p(illum))
     return image, illum, Ps, Psold
+
+
+def image_adjoint(vpp, dh, dt, nt, tlag, rec, Ps, Psold, m, subtract_src=True, w=None, src=0):
+    """Adjoint of backward(..., mode=0) as a map data -> image for the source
+    fields rebuilt from (Ps, Psold): returns data (nrec, nt) such that
+    <backward image(d), m> = <d, image_adjoint(m)>."""
+    vpp = _d64(vpp)
+    nyy, nxx, nzz = vpp.shape
+    rec = np.ascontiguousarray(rec, dtype=np.int64)
+    out = np.zeros((rec.size, nt))
+    w = np.zeros(max(nt, 1)) if w is None else _d64(w)
+    st = load().orc_image_adjoint(nzz, nxx, nyy, dh, dt, nt, tlag, _p(vpp), rec.size, rec.ctypes.data_as(_lp),
+                                  int(subtract_src), _p(w), int(src), _p(_d64(Ps)), _p(_d64(Psold)),
+                                  _p(_d64(m)), _p(out))
+    if st:
+        raise MemoryError("orc_image_adjoint: out of memory")
+    return out
 
 
 def rtm_post(image_pad, illum_pad, nz, nx, ny, nb, dh):

@@ -12,8 +12,8 @@
 // seeded from clock64()/std::random_device and its generator kernels have
 // unguarded tail threads (src/modeling/modeling.cu:594-666), so they are not
 // run.  The backward pass repeats the five-line time loop of
-// Migration::backward_propagation (src/migration/migration.cu:119-127) or
-// Inversion::backward_propagation (src/inversion/inversion.cu:335-343) around
+// Migration::backward_propagation (src/migration/migration.cu:72-80) or
+// Inversion::backward_propagation (src/inversion/inversion.cu:244-252) around
 // the reference's kernels inject_seismogram + cross_correlation or
 // inject_residuo + build_gradient.
 #include <cuda_runtime.h>

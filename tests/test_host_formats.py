@@ -1,5 +1,5 @@
 """The reference's host file formats behind the C ABI (no GPU needed):
-parameters.txt lookup (src/admin/admin.cpp:86-121), SPS/RPS points
+parameters.txt lookup (src/admin/admin.cpp:53-88), SPS/RPS points
 (src/geometry/geometry.cpp:3-47) and raw float32 binaries."""
 import numpy as np
 import pytest

@@ -91,13 +91,13 @@ def test_blob_list_has_the_reference_distributions():
     n = len(b)
     assert n > 1000
     x, y, z, r, amp = b.T.astype(np.float64)
-    # radius U(0.2 r, r), amplitude U(0.5 varVp, varVp) (modeling.cu:583-584)
+    # radius U(0.2 r, r), amplitude U(0.5 varVp, varVp) (modeling.cu:585-586)
     assert r.min() >= 0.2 * ratio * (1 - 1e-6) and r.max() <= ratio * (1 + 1e-6)
     assert abs(r.mean() - 0.6 * ratio) < 4 * (0.8 * ratio / np.sqrt(12)) / np.sqrt(n)
     a = np.abs(amp)
     assert a.min() >= 0.5 * varVp * (1 - 1e-6) and a.max() <= varVp * (1 + 1e-6)
     assert abs(a.mean() - 0.75 * varVp) < 4 * (0.5 * varVp / np.sqrt(12)) / np.sqrt(n)
-    # sign negative with probability 1/3 (rand() % 3 == 0, modeling.cu:586)
+    # sign negative with probability 1/3 (rand() % 3 == 0, modeling.cu:588)
     p = float(np.mean(amp < 0))
     assert abs(p - 1 / 3) < 4 * np.sqrt((1 / 3) * (2 / 3) / n), p
     # centres outside the inner box shrunk by half the pad (modeling.cu:571-577)
