@@ -22,6 +22,9 @@
  *   - One context per host thread; calls on one context are not re-entrant.
  *     Each context owns one CUDA stream (or uses the one set with
  *     fwi_set_stream) and its captured time-loop graphs.
+ *   - The library keeps per-device state for the life of the process (kernel
+ *     attributes, grid sizes, the no-alloc scratch address); cudaDeviceReset
+ *     while it is loaded is not supported.
  */
 #ifndef FWI3D_H
 #define FWI3D_H
