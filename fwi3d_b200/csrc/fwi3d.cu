@@ -51,10 +51,10 @@ KInfo fwd_info(bool abc)
 {
     using T = TileOf<I>;
     KInfo k;
-    k.threads = T::THREADS;
+    k.threads = T::NT;
     k.tz = T::TZ;
     k.tx = T::TX;
-    k.smem = SHF * T::HSLOT + SCF * 2 * T::CSLOT + 2 * (SHF + SCF) * 8;  // rings + full/empty barriers
+    k.smem = SHF * T::HSLOT + SCF * 2 * T::CSLOT + (SHF + SCF) * 8;
     k.fn = abc ? (const void *)fd_forward_kernel<T, SHF, SCF, true>
                : (const void *)fd_forward_kernel<T, SHF, SCF, false>;
     return k;
@@ -65,10 +65,10 @@ KInfo bwd_info(bool grad, bool dy)
 {
     using T = TileOf<I>;
     KInfo k;
-    k.threads = T::THREADS;
+    k.threads = T::NT;
     k.tz = T::TZ;
     k.tx = T::TX;
-    k.smem = SHB * 2 * T::HSLOT + SCB * 5 * T::CSLOT + 2 * (SHB + SCB) * 8;
+    k.smem = SHB * 2 * T::HSLOT + SCB * 5 * T::CSLOT + (SHB + SCB) * 8;
     if (!grad)
         k.fn = (const void *)fd_backward_kernel<T, SHB, SCB, false, false>;
     else if (dy)

@@ -27,15 +27,9 @@
 //     centre of plane y+4.
 //   - Centre-only fields (old time level, velocity, accumulators) arrive as
 //     TZ x TX tiles in a second ring of SC slots.
-//   - Warp specialisation: one producer warp (its lane 0) issues every TMA
-//     copy; the compute warps consume.  Each ring slot has a "full" mbarrier
-//     (the copy's bytes landed) and an "empty" one that every compute warp
-//     arrives on once it has read the slot for the last time; the producer
-//     refills a slot only after its empty phase completed.  There is no
-//     CTA-wide barrier inside the plane loop, so warps drift apart by up to
-//     the ring depth instead of waiting for the slowest one at every plane.
-//   - Every mbarrier wait is bounded (kWaitLimitNs): a warp that gives up
-//     sets g_status and leaves; the producer drains the copies it issued.
+//   - One elected thread issues every TMA copy; completion is tracked with
+//     mbarriers whose waits are bounded (kWaitLimitNs) and report through
+//     g_status instead of hanging.
 #pragma once
 
 #include "device.cuh"
@@ -47,9 +41,7 @@ __device__ unsigned int g_status;
 template <int TZ4_, int TX_>
 struct Tile {
     static constexpr int TZ4 = TZ4_, TX = TX_;
-    static constexpr int NT = TZ4 * TX;          // compute threads
-    static constexpr int NCW = (NT + 31) / 32;   // compute warps
-    static constexpr int THREADS = 32 * (NCW + 1);  // plus one producer warp
+    static constexpr int NT = TZ4 * TX;          // threads
     static constexpr int TZ = 4 * TZ4;           // z cells
     static constexpr int HZ = TZ + 8, HX = TX + 8;
     static constexpr int HALO_BYTES = HZ * HX * 4;
@@ -121,47 +113,6 @@ __global__ void bounded_wait_probe_kernel(uint64_t limit_ns)
 }
 
 // ---------------------------------------------------------------------------
-// Ring bookkeeping shared by both kernels.
-//
-// Halo plane q of [pf, pl] goes to slot (q - pf) % SH; it is read at
-// iteration q (into the y queue) and, when ya <= q < yb, again at iteration
-// q + 4 as the z/x neighbour tile of plane y = q.  Its slot is released after
-// its last read.  Centre plane y of [ya, yb) goes to slot (y - ya) % SC and
-// is read (and released) at iteration y + 4.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ bool wait_use(uint64_t *bars, int i, int depth)
-{
-    return mbar_wait(&bars[i % depth], (i / depth) & 1);
-}
-
-// Producer side: wait until slot (i % depth) is free for its (i / depth)-th use.
-__device__ __forceinline__ bool wait_free(uint64_t *empty, int i, int depth)
-{
-    return i < depth || mbar_wait(&empty[i % depth], ((i / depth) - 1) & 1);
-}
-
-// Consumer side: after iteration p, lane 0 of every compute warp releases the
-// slots read for the last time.
-__device__ __forceinline__ void release_after(int p, int pf, int ya, int yb, int SH, int SC, uint64_t *hempty,
-                                              uint64_t *cempty)
-{
-    const int y = p - 4;
-    if (p < ya || p >= yb) mbar_arrive(&hempty[(p - pf) % SH]);
-    if (y >= ya) {
-        mbar_arrive(&hempty[(y - pf) % SH]);
-        mbar_arrive(&cempty[(y - ya) % SC]);
-    }
-}
-
-// Producer side after a failed wait: the newest copy of every slot may still
-// be in flight into this CTA's shared memory; wait (bounded) for it.
-__device__ __forceinline__ void drain(uint64_t *full, int first, int last, int depth)
-{
-    for (int i = (last - first + 1 > depth ? last - depth + 1 : first); i <= last; ++i)
-        mbar_wait(&full[(i - first) % depth], ((i - first) / depth) & 1);
-}
-
-// ---------------------------------------------------------------------------
 // Forward leapfrog step.
 //   mh: halo-box map over A (the field read with the stencil)
 //   mq: centre-box map over Q (the field overwritten)
@@ -169,7 +120,7 @@ __device__ __forceinline__ void drain(uint64_t *full, int first, int last, int d
 //       shot, or one slot per shot when every shot has its own random pad)
 // ---------------------------------------------------------------------------
 template <class T, int SH, int SC, bool ABC>
-__global__ void __launch_bounds__(T::THREADS, T::THREADS <= 384 ? 2 : 1)
+__global__ void __launch_bounds__(T::NT)
     fd_forward_kernel(const __grid_constant__ CUtensorMap mh, const __grid_constant__ CUtensorMap mq,
                       const __grid_constant__ CUtensorMap mv, const FwdArgs a)
 {
@@ -177,14 +128,12 @@ __global__ void __launch_bounds__(T::THREADS, T::THREADS <= 384 ? 2 : 1)
     extern __shared__ __align__(128) unsigned char smem[];
     unsigned char *hring = smem;
     unsigned char *cring = smem + SH * T::HSLOT;
-    uint64_t *hfull = reinterpret_cast<uint64_t *>(cring + SC * 2 * T::CSLOT);
-    uint64_t *hempty = hfull + SH;
-    uint64_t *cfull = hempty + SH;
-    uint64_t *cempty = cfull + SC;
+    uint64_t *hbar = reinterpret_cast<uint64_t *>(cring + SC * 2 * T::CSLOT);
+    uint64_t *cbar = hbar + SH;
     __shared__ float b1s[ABC ? kMaxPad : 1];
+    __shared__ int abort_flag;
 
     const int tid = threadIdx.x;
-    const int warp = tid >> 5, lane = tid & 31;
     const int shot = blockIdx.y;
     if (status_failed()) return;
 
@@ -193,8 +142,8 @@ __global__ void __launch_bounds__(T::THREADS, T::THREADS <= 384 ? 2 : 1)
     // in-place damping, i.e. d * A (src/modeling/modeling.cu:378, 391-392).
     if (a.t > a.tlag) {
         const int R = a.binfo->R;
-        const long long total = (long long)gridDim.x * gridDim.y * blockDim.x;
-        for (long long g = ((long long)blockIdx.y * gridDim.x + blockIdx.x) * blockDim.x + tid; g < R;
+        const long long total = (long long)gridDim.x * gridDim.y * T::NT;
+        for (long long g = ((long long)blockIdx.y * gridDim.x + blockIdx.x) * T::NT + tid; g < R;
              g += total)
             a.seis_tm[(long long)(a.t - a.tlag) * R + g] = a.rec_damp[g] * a.A[a.rec_cell[g]];
     }
@@ -208,65 +157,48 @@ __global__ void __launch_bounds__(T::THREADS, T::THREADS <= 384 ? 2 : 1)
     const int ya = 4 + ch * a.ylen;
     const int yb = min(ya + a.ylen, a.nyy - 4);
     if (ya >= yb || shot >= a.binfo->nshot) return;  // uniform per CTA
+
+    const int lz = tid % T::TZ4, lx = tid / T::TZ4;
+    const int zc = z0 + 4 * lz, xc = x0 + lx;
     const int vshot = a.vel_slots > 1 ? shot : 0;
-    const int pf = ya - 4, pl = yb + 3;  // halo planes loaded: [pf, pl]
 
     if constexpr (ABC) {
-        for (int i = tid; i < a.nb; i += blockDim.x) b1s[i] = a.b1d[i];
+        for (int i = tid; i < a.nb; i += T::NT) b1s[i] = a.b1d[i];
     }
     if (tid == 0) {
-        for (int s = 0; s < SH; ++s) {
-            mbar_init(&hfull[s], 1);
-            mbar_init(&hempty[s], T::NCW);
-        }
-        for (int s = 0; s < SC; ++s) {
-            mbar_init(&cfull[s], 1);
-            mbar_init(&cempty[s], T::NCW);
-        }
+        abort_flag = 0;
+        prefetch_tmap(&mh);
+        prefetch_tmap(&mq);
+        prefetch_tmap(&mv);
+        for (int s = 0; s < SH; ++s) mbar_init(&hbar[s], 1);
+        for (int s = 0; s < SC; ++s) mbar_init(&cbar[s], 1);
         fence_mbar_init();
     }
     __syncthreads();
 
-    if (warp == T::NCW) {
-        // ---- producer: copies in the order the compute warps need them ----
-        if (lane != 0) return;
-        prefetch_tmap(&mh);
-        prefetch_tmap(&mq);
-        prefetch_tmap(&mv);
-        int h_issued = pf - 1, c_issued = ya - 1;
-        bool ok = true;
-        for (int p = pf; p <= pl; ++p) {
-            const int ih = p - pf;
-            if (!(ok = wait_free(hempty, ih, SH))) break;
-            fence_proxy_async();
-            mbar_expect_tx(&hfull[ih % SH], T::HALO_BYTES);
-            tma_load_4d(hring + (ih % SH) * T::HSLOT, &mh, &hfull[ih % SH], z0 - 4, x0 - 4, p, shot);
-            h_issued = p;
-            const int y = p - 4;
-            if (y < ya) continue;
-            const int ic = y - ya;
-            if (!(ok = wait_free(cempty, ic, SC))) break;
-            fence_proxy_async();
-            mbar_expect_tx(&cfull[ic % SC], 2 * T::CTR_BYTES);
-            tma_load_4d(cring + (2 * (ic % SC)) * T::CSLOT, &mq, &cfull[ic % SC], z0, x0, y, shot);
-            tma_load_4d(cring + (2 * (ic % SC) + 1) * T::CSLOT, &mv, &cfull[ic % SC], z0, x0, y, vshot);
-            c_issued = y;
-        }
-        if (!ok) {
-            raise_status(kErrTimeout);
-            drain(hfull, pf, h_issued, SH);
-            drain(cfull, ya, c_issued, SC);
-        }
-        return;
+    const int pf = ya - 4, pl = yb + 3;  // halo planes loaded: [pf, pl]
+    int h_issued = pf - 1, c_issued = ya - 1;  // meaningful in thread 0 only
+    auto issue_h = [&](int p) {
+        const int s = (p - pf) % SH;
+        mbar_expect_tx(&hbar[s], T::HALO_BYTES);
+        tma_load_4d(hring + s * T::HSLOT, &mh, &hbar[s], z0 - 4, x0 - 4, p, shot);
+        h_issued = p;
+    };
+    auto issue_c = [&](int y) {
+        const int s = (y - ya) % SC;
+        mbar_expect_tx(&cbar[s], 2 * T::CTR_BYTES);
+        tma_load_4d(cring + (2 * s) * T::CSLOT, &mq, &cbar[s], z0, x0, y, shot);
+        tma_load_4d(cring + (2 * s + 1) * T::CSLOT, &mv, &cbar[s], z0, x0, y, vshot);
+        c_issued = y;
+    };
+    if (tid == 0) {
+        for (int p = pf; p < pf + SH && p <= pl; ++p) issue_h(p);
+        for (int y = ya; y < ya + SC && y < yb; ++y) issue_c(y);
     }
 
-    // ---- compute warps ----
-    const bool active = tid < T::NT;
-    const int lz = tid % T::TZ4, lx = tid / T::TZ4;
-    const int zc = z0 + 4 * lz, xc = x0 + lx;
     const int3 src = make_int3(a.binfo->src[shot][0], a.binfo->src[shot][1], a.binfo->src[shot][2]);
     const int ro = (lx + 4) * T::HZ, zo = 4 + 4 * lz;
-    const bool row_ok = active && xc < a.nxx - 4 && zc < a.nzz - 4;
+    const bool row_ok = xc < a.nxx - 4 && zc < a.nzz - 4;
     const int dx = ABC ? pad_depth(xc, a.nxx, a.nb) : -1;
     float *Qshot = a.Q + (long long)shot * a.vol;
     const long long plane = (long long)a.ldz * a.nxx;
@@ -277,19 +209,16 @@ __global__ void __launch_bounds__(T::THREADS, T::THREADS <= 384 ? 2 : 1)
 
     for (int p = pf; p <= pl; ++p) {
         const int y = p - 4;
-        bool ok = wait_use(hfull, p - pf, SH);
-        if (y >= ya) ok = wait_use(cfull, y - ya, SC) && ok;
-        if (!__all_sync(0xffffffffu, ok)) {
-            if (lane == 0) raise_status(kErrTimeout);
-            break;
-        }
-        if (active) {
-            const float *Hp = reinterpret_cast<const float *>(hring + ((p - pf) % SH) * T::HSLOT);
+        bool ok = mbar_wait(&hbar[(p - pf) % SH], ((p - pf) / SH) & 1);
+        if (y >= ya) ok = mbar_wait(&cbar[(y - ya) % SC], ((y - ya) / SC) & 1) && ok;
+        if (!ok) abort_flag = 1;
+
+        const float *Hp = reinterpret_cast<const float *>(hring + ((p - pf) % SH) * T::HSLOT);
 #pragma unroll
-            for (int m = 0; m < 8; ++m) q[m] = q[m + 1];
-            q[8] = lds4(Hp + ro + zo);
-        }
-        if (active && y >= ya) {
+        for (int m = 0; m < 8; ++m) q[m] = q[m + 1];
+        q[8] = lds4(Hp + ro + zo);
+
+        if (y >= ya) {
             const float *Hy = reinterpret_cast<const float *>(hring + ((y - pf) % SH) * T::HSLOT);
             const int cs = (y - ya) % SC;
             const float *Cq = reinterpret_cast<const float *>(cring + (2 * cs) * T::CSLOT);
@@ -328,8 +257,24 @@ __global__ void __launch_bounds__(T::THREADS, T::THREADS <= 384 ? 2 : 1)
             if (row_ok)
                 *reinterpret_cast<float4 *>(Qshot + y * plane + (long long)xc * a.ldz + zc) = out;
         }
-        __syncwarp();
-        if (lane == 0) release_after(p, pf, ya, yb, SH, SC, hempty, cempty);
+        __syncthreads();
+        if (abort_flag) break;
+        if (tid == 0) {
+            fence_proxy_async();
+            if (p < ya) {
+                if (p + SH <= pl) issue_h(p + SH);
+            } else if (y >= ya) {
+                if (y + SH <= pl) issue_h(y + SH);
+                if (y + SC < yb) issue_c(y + SC);
+            }
+        }
+    }
+
+    if (abort_flag && tid == 0) {
+        raise_status(kErrTimeout);
+        // Drain copies still in flight into this CTA's shared memory.
+        for (int p = pf; p <= h_issued; ++p) mbar_wait(&hbar[(p - pf) % SH], ((p - pf) / SH) & 1);
+        for (int y = ya; y <= c_issued; ++y) mbar_wait(&cbar[(y - ya) % SC], ((y - ya) / SC) & 1);
     }
 }
 
@@ -342,7 +287,7 @@ __global__ void __launch_bounds__(T::THREADS, T::THREADS <= 384 ? 2 : 1)
 // GRAD: gradient imaging condition (with GRAD_DY the d2y term is kept).
 // ---------------------------------------------------------------------------
 template <class T, int SH, int SC, bool GRAD, bool GRAD_DY>
-__global__ void __launch_bounds__(T::THREADS)
+__global__ void __launch_bounds__(T::NT)
     fd_backward_kernel(const __grid_constant__ CUtensorMap mhs, const __grid_constant__ CUtensorMap mhr,
                        const __grid_constant__ CUtensorMap mcs, const __grid_constant__ CUtensorMap mcr,
                        const __grid_constant__ CUtensorMap mv, const __grid_constant__ CUtensorMap mim,
@@ -353,13 +298,11 @@ __global__ void __launch_bounds__(T::THREADS)
     extern __shared__ __align__(128) unsigned char smem[];
     unsigned char *hring = smem;                            // SH x {Psold, Pr}
     unsigned char *cring = smem + SH * 2 * T::HSLOT;        // SC x {Ps, Prold, v, img, ill}
-    uint64_t *hfull = reinterpret_cast<uint64_t *>(cring + SC * NCF * T::CSLOT);
-    uint64_t *hempty = hfull + SH;
-    uint64_t *cfull = hempty + SH;
-    uint64_t *cempty = cfull + SC;
+    uint64_t *hbar = reinterpret_cast<uint64_t *>(cring + SC * NCF * T::CSLOT);
+    uint64_t *cbar = hbar + SH;
+    __shared__ int abort_flag;
 
     const int tid = threadIdx.x;
-    const int warp = tid >> 5, lane = tid & 31;
     const int shot = blockIdx.y;
     if (status_failed()) return;
     int b = blockIdx.x;
@@ -371,69 +314,52 @@ __global__ void __launch_bounds__(T::THREADS)
     const int ya = 4 + ch * a.ylen;
     const int yb = min(ya + a.ylen, a.nyy - 4);
     if (ya >= yb || shot >= a.binfo->nshot) return;
+
+    const int lz = tid % T::TZ4, lx = tid / T::TZ4;
+    const int zc = z0 + 4 * lz, xc = x0 + lx;
     const int vshot = a.vel_slots > 1 ? shot : 0;
-    const int pf = ya - 4, pl = yb + 3;
 
     if (tid == 0) {
-        for (int s = 0; s < SH; ++s) {
-            mbar_init(&hfull[s], 1);
-            mbar_init(&hempty[s], T::NCW);
-        }
-        for (int s = 0; s < SC; ++s) {
-            mbar_init(&cfull[s], 1);
-            mbar_init(&cempty[s], T::NCW);
-        }
+        abort_flag = 0;
+        prefetch_tmap(&mhs);
+        prefetch_tmap(&mhr);
+        for (int s = 0; s < SH; ++s) mbar_init(&hbar[s], 1);
+        for (int s = 0; s < SC; ++s) mbar_init(&cbar[s], 1);
         fence_mbar_init();
     }
     __syncthreads();
 
-    if (warp == T::NCW) {
-        // ---- producer ----
-        if (lane != 0) return;
-        prefetch_tmap(&mhs);
-        prefetch_tmap(&mhr);
-        int h_issued = pf - 1, c_issued = ya - 1;
-        bool ok = true;
-        for (int p = pf; p <= pl; ++p) {
-            const int ih = p - pf, hs = ih % SH;
-            if (!(ok = wait_free(hempty, ih, SH))) break;
-            fence_proxy_async();
-            mbar_expect_tx(&hfull[hs], 2 * T::HALO_BYTES);
-            tma_load_4d(hring + (2 * hs) * T::HSLOT, &mhs, &hfull[hs], z0 - 4, x0 - 4, p, shot);
-            tma_load_4d(hring + (2 * hs + 1) * T::HSLOT, &mhr, &hfull[hs], z0 - 4, x0 - 4, p, shot);
-            h_issued = p;
-            const int y = p - 4;
-            if (y < ya) continue;
-            const int ic = y - ya, cs = ic % SC;
-            if (!(ok = wait_free(cempty, ic, SC))) break;
-            fence_proxy_async();
-            unsigned char *base = cring + cs * NCF * T::CSLOT;
-            mbar_expect_tx(&cfull[cs], NCF * T::CTR_BYTES);
-            tma_load_4d(base + 0 * T::CSLOT, &mcs, &cfull[cs], z0, x0, y, shot);
-            tma_load_4d(base + 1 * T::CSLOT, &mcr, &cfull[cs], z0, x0, y, shot);
-            tma_load_4d(base + 2 * T::CSLOT, &mv, &cfull[cs], z0, x0, y, vshot);
-            tma_load_4d(base + 3 * T::CSLOT, &mim, &cfull[cs], z0, x0, y, shot);
-            tma_load_4d(base + 4 * T::CSLOT, &mil, &cfull[cs], z0, x0, y, shot);
-            c_issued = y;
-        }
-        if (!ok) {
-            raise_status(kErrTimeout);
-            drain(hfull, pf, h_issued, SH);
-            drain(cfull, ya, c_issued, SC);
-        }
-        return;
+    const int pf = ya - 4, pl = yb + 3;
+    int h_issued = pf - 1, c_issued = ya - 1;
+    auto issue_h = [&](int p) {
+        const int s = (p - pf) % SH;
+        mbar_expect_tx(&hbar[s], 2 * T::HALO_BYTES);
+        tma_load_4d(hring + (2 * s) * T::HSLOT, &mhs, &hbar[s], z0 - 4, x0 - 4, p, shot);
+        tma_load_4d(hring + (2 * s + 1) * T::HSLOT, &mhr, &hbar[s], z0 - 4, x0 - 4, p, shot);
+        h_issued = p;
+    };
+    auto issue_c = [&](int y) {
+        const int s = (y - ya) % SC;
+        unsigned char *base = cring + s * NCF * T::CSLOT;
+        mbar_expect_tx(&cbar[s], NCF * T::CTR_BYTES);
+        tma_load_4d(base + 0 * T::CSLOT, &mcs, &cbar[s], z0, x0, y, shot);
+        tma_load_4d(base + 1 * T::CSLOT, &mcr, &cbar[s], z0, x0, y, shot);
+        tma_load_4d(base + 2 * T::CSLOT, &mv, &cbar[s], z0, x0, y, vshot);
+        tma_load_4d(base + 3 * T::CSLOT, &mim, &cbar[s], z0, x0, y, shot);
+        tma_load_4d(base + 4 * T::CSLOT, &mil, &cbar[s], z0, x0, y, shot);
+        c_issued = y;
+    };
+    if (tid == 0) {
+        for (int p = pf; p < pf + SH && p <= pl; ++p) issue_h(p);
+        for (int y = ya; y < ya + SC && y < yb; ++y) issue_c(y);
     }
 
-    // ---- compute warps ----
-    const bool active = tid < T::NT;
-    const int lz = tid % T::TZ4, lx = tid / T::TZ4;
-    const int zc = z0 + 4 * lz, xc = x0 + lx;
     const int3 src = make_int3(a.binfo->src[shot][0], a.binfo->src[shot][1], a.binfo->src[shot][2]);
     // Stored field A_{N-t} carried source sample N-t; the exact rebuild adds it back.
     const float scorr = (a.subtract_src && a.nsteps - a.t < a.nt)
                             ? a.idh3 * a.wavelet[a.nsteps - a.t] : 0.0f;
     const int ro = (lx + 4) * T::HZ, zo = 4 + 4 * lz;
-    const bool row_ok = active && xc < a.nxx - 4 && zc < a.nzz - 4;
+    const bool row_ok = xc < a.nxx - 4 && zc < a.nzz - 4;
     const long long plane = (long long)a.ldz * a.nxx;
     const long long sh_off = (long long)shot * a.vol;
 
@@ -446,25 +372,22 @@ __global__ void __launch_bounds__(T::THREADS)
 
     for (int p = pf; p <= pl; ++p) {
         const int y = p - 4;
-        bool ok = wait_use(hfull, p - pf, SH);
-        if (y >= ya) ok = wait_use(cfull, y - ya, SC) && ok;
-        if (!__all_sync(0xffffffffu, ok)) {
-            if (lane == 0) raise_status(kErrTimeout);
-            break;
-        }
-        if (active) {
-            const int hs = (p - pf) % SH;
-            const float *Hs = reinterpret_cast<const float *>(hring + (2 * hs) * T::HSLOT);
-            const float *Hr = reinterpret_cast<const float *>(hring + (2 * hs + 1) * T::HSLOT);
+        bool ok = mbar_wait(&hbar[(p - pf) % SH], ((p - pf) / SH) & 1);
+        if (y >= ya) ok = mbar_wait(&cbar[(y - ya) % SC], ((y - ya) / SC) & 1) && ok;
+        if (!ok) abort_flag = 1;
+
+        const int hs = (p - pf) % SH;
+        const float *Hs = reinterpret_cast<const float *>(hring + (2 * hs) * T::HSLOT);
+        const float *Hr = reinterpret_cast<const float *>(hring + (2 * hs + 1) * T::HSLOT);
 #pragma unroll
-            for (int m = 0; m < 8; ++m) {
-                qs[m] = qs[m + 1];
-                qr[m] = qr[m + 1];
-            }
-            qs[8] = lds4(Hs + ro + zo);
-            qr[8] = lds4(Hr + ro + zo);
+        for (int m = 0; m < 8; ++m) {
+            qs[m] = qs[m + 1];
+            qr[m] = qr[m + 1];
         }
-        if (active && y >= ya) {
+        qs[8] = lds4(Hs + ro + zo);
+        qr[8] = lds4(Hr + ro + zo);
+
+        if (y >= ya) {
             const int hy = (y - pf) % SH;
             const float *Hys = reinterpret_cast<const float *>(hring + (2 * hy) * T::HSLOT);
             const float *Hyr = reinterpret_cast<const float *>(hring + (2 * hy + 1) * T::HSLOT);
@@ -528,8 +451,23 @@ __global__ void __launch_bounds__(T::THREADS)
                 *reinterpret_cast<float4 *>(a.illum + off) = ill;
             }
         }
-        __syncwarp();
-        if (lane == 0) release_after(p, pf, ya, yb, SH, SC, hempty, cempty);
+        __syncthreads();
+        if (abort_flag) break;
+        if (tid == 0) {
+            fence_proxy_async();
+            if (p < ya) {
+                if (p + SH <= pl) issue_h(p + SH);
+            } else if (y >= ya) {
+                if (y + SH <= pl) issue_h(y + SH);
+                if (y + SC < yb) issue_c(y + SC);
+            }
+        }
+    }
+
+    if (abort_flag && tid == 0) {
+        raise_status(kErrTimeout);
+        for (int p = pf; p <= h_issued; ++p) mbar_wait(&hbar[(p - pf) % SH], ((p - pf) / SH) & 1);
+        for (int y = ya; y <= c_issued; ++y) mbar_wait(&cbar[(y - ya) % SC], ((y - ya) / SC) & 1);
     }
 }
 
