@@ -1188,14 +1188,28 @@ void grow_velocity_slots(fwi_ctx *c, int n)
     ++c->generation;
 }
 
-// Per-shot random pads of one batch (shots ids[0..n)), then the blob sets
-// of the next batch's shots start building on host threads.
+// Per-shot random pads of one batch (shots ids[0..n)).  The batch's blob sets
+// build on host threads side by side, and so do those of the next batch
+// while the GPU propagates this one: the next shots of this call when there
+// are any, otherwise the shots that continue this batch's stride (the next
+// call's batch when shots come in order; a wrong guess only costs host time).
 void shot_pads(fwi_ctx *c, const int *ids, int n, const int *next, int n_next)
 {
-    for (int k = 0; k < n; ++k) pad_slot(c, &c->shot_rbc_params, c->shot_rbc_seed + (uint64_t)ids[k], c->vel_slots > 1 ? k : 0);
-    if (wants_blobs(&c->shot_rbc_params))
-        for (int k = 0; k < n_next; ++k)
-            c->blob_cache.prefetch(blob_key(c, &c->shot_rbc_params, c->shot_rbc_seed + (uint64_t)next[k]));
+    const fwi_rbc *rbc = &c->shot_rbc_params;
+    if (wants_blobs(rbc)) {
+        auto want = [&](int shot) { c->blob_cache.prefetch(blob_key(c, rbc, c->shot_rbc_seed + (uint64_t)shot)); };
+        for (int k = 0; k < n; ++k) want(ids[k]);
+        if (n_next > 0) {
+            for (int k = 0; k < n_next; ++k) want(next[k]);
+        } else {
+            const int stride = n > 1 ? ids[n - 1] - ids[n - 2] : 1;
+            for (int k = 1; k <= c->B && stride > 0; ++k) {
+                const long long s = ids[n - 1] + (long long)k * stride;
+                if (s < c->nsrc) want((int)s);
+            }
+        }
+    }
+    for (int k = 0; k < n; ++k) pad_slot(c, rbc, c->shot_rbc_seed + (uint64_t)ids[k], c->vel_slots > 1 ? k : 0);
     // synchronises the stream: the slots' host blob copies outlive their uploads
     check_cfl(c, c->vel_slots > 1 ? n : 1);
 }
@@ -1791,60 +1805,66 @@ int fwi_autotune(fwi_ctx *c)
         t.info.R = 0;
         t.info.ncell = 0;
         upload_batch(c, t);
-        const int steps = 6;
+        // Candidates: every compiled tile x three y-chunk counts.  Each is timed
+        // over kSteps launches after one warm launch, in two passes (the SM
+        // clock moves under the power cap during a sweep), and keeps its faster
+        // pass.  The heuristic default stays unless a candidate beats it by
+        // more than 1 %: a short window can favour whatever ran while the
+        // clock was high.
+        constexpr int kSteps = 12, kPasses = 2;
         cudaEvent_t e0, e1;
         CK(cudaEventCreate(&e0));
         CK(cudaEventCreate(&e1));
-        float best = 1e30f;
-        int best_tile = 0, best_chunk = 1;
-        for (int tile = 0; tile < kNumTiles; ++tile) {
-            KInfo k = fwd_kernel(tile, !adj);
-            const int base = default_chunks(c, k, c->B);
-            for (int nchunk : {base, std::max(1, base / 2), base * 2}) {
-                FwdLaunch L = make_fwd(c, c->B, tile, nchunk, false);
-                launch_fwd(c, L, 0, 0);
-                CK(cudaEventRecord(e0, c->stream));
-                for (int s = 0; s < steps; ++s) launch_fwd(c, L, 1, s & 1);
-                CK(cudaEventRecord(e1, c->stream));
-                CK(cudaEventSynchronize(e1));
-                float ms = 0;
-                CK(cudaEventElapsedTime(&ms, e0, e1));
-                c->launches += steps + 1;
-                if (ms < best) {
-                    best = ms;
-                    best_tile = tile;
-                    best_chunk = nchunk;
-                }
-            }
-        }
-        c->tile_fwd = best_tile;
-        c->chunk_fwd = best_chunk;
-        if (adj) {
-            best = 1e30f;
-            best_tile = 0;
-            best_chunk = 1;
+        struct Cand {
+            int tile, nchunk;
+            float ms;
+        };
+        auto tune = [&](bool backward, int &tile_out, int &chunk_out) {
+            std::vector<Cand> cands;
             for (int tile = 0; tile < kNumTiles; ++tile) {
-                KInfo k = bwd_kernel(tile, false, false);
+                const KInfo k = backward ? bwd_kernel(tile, false, false) : fwd_kernel(tile, !adj);
                 const int base = default_chunks(c, k, c->B);
                 for (int nchunk : {base, std::max(1, base / 2), base * 2}) {
-                    BwdLaunch L = make_bwd(c, c->B, tile, nchunk, false);
-                    launch_bwd(c, L, 0, 0, 0);
-                    CK(cudaEventRecord(e0, c->stream));
-                    for (int s = 0; s < steps; ++s) launch_bwd(c, L, 1, s & 1, s & 1);
+                    bool dup = false;
+                    for (const Cand &q : cands) dup |= q.tile == tile && q.nchunk == nchunk;
+                    if (!dup) cands.push_back({tile, nchunk, 1e30f});
+                }
+            }
+            for (int pass = 0; pass < kPasses; ++pass) {
+                for (Cand &q : cands) {
+                    if (backward) {
+                        BwdLaunch L = make_bwd(c, c->B, q.tile, q.nchunk, false);
+                        launch_bwd(c, L, 0, 0, 0);
+                        CK(cudaEventRecord(e0, c->stream));
+                        for (int s = 0; s < kSteps; ++s) launch_bwd(c, L, 1, s & 1, s & 1);
+                    } else {
+                        FwdLaunch L = make_fwd(c, c->B, q.tile, q.nchunk, false);
+                        launch_fwd(c, L, 0, 0);
+                        CK(cudaEventRecord(e0, c->stream));
+                        for (int s = 0; s < kSteps; ++s) launch_fwd(c, L, 1, s & 1);
+                    }
                     CK(cudaEventRecord(e1, c->stream));
                     CK(cudaEventSynchronize(e1));
                     float ms = 0;
                     CK(cudaEventElapsedTime(&ms, e0, e1));
-                    c->launches += steps + 1;
-                    if (ms < best) {
-                        best = ms;
-                        best_tile = tile;
-                        best_chunk = nchunk;
-                    }
+                    q.ms = std::min(q.ms, ms);
+                    c->launches += kSteps + 1;
                 }
             }
-            c->tile_bwd = best_tile;
-            c->chunk_bwd = best_chunk;
+            const Cand *best = &cands[0];
+            for (const Cand &q : cands)
+                if (q.ms < best->ms) best = &q;
+            const int dt = default_tile(c, backward);
+            const KInfo dk = backward ? bwd_kernel(dt, false, false) : fwd_kernel(dt, !adj);
+            const int dc = default_chunks(c, dk, c->B);
+            for (const Cand &q : cands)
+                if (q.tile == dt && q.nchunk == dc && q.ms <= best->ms * 1.01f) best = &q;
+            tile_out = best->tile;
+            chunk_out = best->nchunk;
+        };
+        tune(false, c->tile_fwd, c->chunk_fwd);
+        if (adj) {
+            tune(true, c->tile_bwd, c->chunk_bwd);
             // tuning ran the imaging condition on scratch data
             const size_t bytes = (size_t)c->B * c->vol * sizeof(float);
             CK(cudaMemsetAsync(c->acc_img.p, 0, bytes, c->stream));
