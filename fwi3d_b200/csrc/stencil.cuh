@@ -32,8 +32,6 @@
 //     g_status instead of hanging.
 #pragma once
 
-#include <type_traits>
-
 #include "device.cuh"
 
 namespace fwi {
@@ -68,15 +66,14 @@ __device__ __forceinline__ float d2(float c, float m1, float p1, float m2, float
 }
 
 // Per-axis second derivatives of 4 consecutive z cells of one thread.
-// H: halo tile of the plane (row stride HZ); q: register queue whose window
-// q[O..O+8] holds the plane's y column (q[O+4] = centre).
-template <class T, int O>
-__device__ __forceinline__ void axis_d2(const float *H, int ro, int zo, const float4 (&q)[10],
+// H: halo tile of the plane (row stride HZ); q: register queue (q[4] = centre).
+template <class T>
+__device__ __forceinline__ void axis_d2(const float *H, int ro, int zo, const float4 (&q)[9],
                                         float (&ax)[4], float (&ay)[4], float (&az)[4])
 {
     const float4 zm = lds4(H + ro + zo - 4);
     const float4 zp = lds4(H + ro + zo + 4);
-    const float4 c = q[O + 4];
+    const float4 c = q[4];
     const float w[12] = {zm.x, zm.y, zm.z, zm.w, c.x, c.y, c.z, c.w, zp.x, zp.y, zp.z, zp.w};
     float4 xm[4], xp[4];
 #pragma unroll
@@ -89,8 +86,8 @@ __device__ __forceinline__ void axis_d2(const float *H, int ro, int zo, const fl
         const float c0 = w[4 + e];
         ax[e] = d2(c0, comp(xm[0], e), comp(xp[0], e), comp(xm[1], e), comp(xp[1], e),
                    comp(xm[2], e), comp(xp[2], e), comp(xm[3], e), comp(xp[3], e));
-        ay[e] = d2(c0, comp(q[O + 3], e), comp(q[O + 5], e), comp(q[O + 2], e), comp(q[O + 6], e),
-                   comp(q[O + 1], e), comp(q[O + 7], e), comp(q[O + 0], e), comp(q[O + 8], e));
+        ay[e] = d2(c0, comp(q[3], e), comp(q[5], e), comp(q[2], e), comp(q[6], e), comp(q[1], e),
+                   comp(q[7], e), comp(q[0], e), comp(q[8], e));
         az[e] = d2(c0, w[3 + e], w[5 + e], w[2 + e], w[6 + e], w[1 + e], w[7 + e], w[e], w[8 + e]);
     }
 }
@@ -127,7 +124,7 @@ __global__ void __launch_bounds__(T::NT)
     fd_forward_kernel(const __grid_constant__ CUtensorMap mh, const __grid_constant__ CUtensorMap mq,
                       const __grid_constant__ CUtensorMap mv, const FwdArgs a)
 {
-    static_assert(SH >= 6, "planes p-4 .. p+1 are read in one iteration");
+    static_assert(SH >= 5, "plane y needs halo slots y..y+4");
     extern __shared__ __align__(128) unsigned char smem[];
     unsigned char *hring = smem;
     unsigned char *cring = smem + SH * T::HSLOT;
@@ -194,14 +191,10 @@ __global__ void __launch_bounds__(T::NT)
         tma_load_4d(cring + (2 * s + 1) * T::CSLOT, &mv, &cbar[s], z0, x0, y, vshot);
         c_issued = y;
     };
-    // Halo plane q reuses the slot of plane q - SH once no thread reads that
-    // plane any more (h_free = the highest such plane); centre plane y the
-    // slot of y - SC (c_free).
-    auto refill = [&](int h_free, int c_free) {
-        while (h_issued < pl && h_issued + 1 - SH <= h_free) issue_h(h_issued + 1);
-        while (c_issued < yb - 1 && c_issued + 1 - SC <= c_free) issue_c(c_issued + 1);
-    };
-    if (tid == 0) refill(pf - 1, ya - 1);
+    if (tid == 0) {
+        for (int p = pf; p < pf + SH && p <= pl; ++p) issue_h(p);
+        for (int y = ya; y < ya + SC && y < yb; ++y) issue_c(y);
+    }
 
     const int3 src = make_int3(a.binfo->src[shot][0], a.binfo->src[shot][1], a.binfo->src[shot][2]);
     const int ro = (lx + 4) * T::HZ, zo = 4 + 4 * lz;
@@ -210,92 +203,78 @@ __global__ void __launch_bounds__(T::NT)
     float *Qshot = a.Q + (long long)shot * a.vol;
     const long long plane = (long long)a.ldz * a.nxx;
 
-    // One output plane y from the queue window q[O..O+8] (y - 4 .. y + 4).
-    auto step_plane = [&](auto O_, int y, const float4 (&q)[10]) {
-        constexpr int O = decltype(O_)::value;
-        const float *Hy = reinterpret_cast<const float *>(hring + ((y - pf) % SH) * T::HSLOT);
-        const int cs = (y - ya) % SC;
-        const float *Cq = reinterpret_cast<const float *>(cring + (2 * cs) * T::CSLOT);
-        const float *Cv = reinterpret_cast<const float *>(cring + (2 * cs + 1) * T::CSLOT);
-        float ax[4], ay[4], az[4];
-        axis_d2<T, O>(Hy, ro, zo, q, ax, ay, az);
-        const float4 qo = lds4(Cq + lx * T::TZ + 4 * lz);
-        const float4 vv = lds4(Cv + lx * T::TZ + 4 * lz);
-        const int dy = ABC ? pad_depth(y, a.nyy, a.nb) : -1;
-        float4 out;
+    float4 q[9];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const float v = comp(vv, e);
-            const float cv = v * v * a.cvel;
-            const float lap = ax[e] + ay[e] + az[e];
-            const float p0 = comp(q[O + 4], e);
-            float old = comp(qo, e);
-            float d = 1.0f;
-            if constexpr (ABC) {
-                d = cerjan(b1s, pad_depth(zc + e, a.nzz, a.nb), dx, dy);
-                old = __fmul_rn(d, old);
-            }
-            float nv = fmaf(cv, lap, 2.0f * p0 - old);
-            if constexpr (ABC) nv = __fmul_rn(d, nv);
-            if (zc + e >= a.nzz - 4) nv = comp(qo, e);
-            set_comp(out, e, nv);
-        }
-        // Source sample t+1 goes into the new field, which is exactly where
-        // the reference adds it at the start of the next step
-        // (src/modeling/modeling.cu:347-348).
-        if (y == src.z && xc == src.y) {
-            const int e = src.x - zc;
-            if (e >= 0 && e < 4 && a.t + 1 < a.nt)
-                set_comp(out, e, comp(out, e) + a.idh3 * a.wavelet[a.t + 1]);
-        }
-        if (row_ok) *reinterpret_cast<float4 *>(Qshot + y * plane + (long long)xc * a.ldz + zc) = out;
-    };
+    for (int m = 0; m < 9; ++m) q[m] = make_float4(0.f, 0.f, 0.f, 0.f);
 
-    // Two planes per iteration: halo planes p, p+1 enter the y queue and
-    // output planes y0 = p-4, y1 = p-3 are computed from windows q[0..8] and
-    // q[1..9]; the queue then moves by two (half the register moves and half
-    // the CTA barriers of one plane per iteration).
-    float4 q[10];
-#pragma unroll
-    for (int m = 0; m < 10; ++m) q[m] = make_float4(0.f, 0.f, 0.f, 0.f);
-
-    for (int p = pf; p <= pl; p += 2) {
-        const bool two = p + 1 <= pl;
-        const int y0 = p - 4, y1 = p - 3;
-        const bool o0 = y0 >= ya, o1 = two && y1 >= ya;  // y0, y1 < yb as p + 1 <= pl = yb + 3
+    for (int p = pf; p <= pl; ++p) {
+        const int y = p - 4;
         bool ok = mbar_wait(&hbar[(p - pf) % SH], ((p - pf) / SH) & 1);
-        if (two) ok = mbar_wait(&hbar[(p + 1 - pf) % SH], ((p + 1 - pf) / SH) & 1) && ok;
-        if (o0) ok = mbar_wait(&cbar[(y0 - ya) % SC], ((y0 - ya) / SC) & 1) && ok;
-        if (o1) ok = mbar_wait(&cbar[(y1 - ya) % SC], ((y1 - ya) / SC) & 1) && ok;
+        if (y >= ya) ok = mbar_wait(&cbar[(y - ya) % SC], ((y - ya) / SC) & 1) && ok;
         if (!ok) abort_flag = 1;
 
-        q[8] = lds4(reinterpret_cast<const float *>(hring + ((p - pf) % SH) * T::HSLOT) + ro + zo);
-        if (two) q[9] = lds4(reinterpret_cast<const float *>(hring + ((p + 1 - pf) % SH) * T::HSLOT) + ro + zo);
-        if (o0) step_plane(std::integral_constant<int, 0>{}, y0, q);
-        if (o1) step_plane(std::integral_constant<int, 1>{}, y1, q);
+        const float *Hp = reinterpret_cast<const float *>(hring + ((p - pf) % SH) * T::HSLOT);
 #pragma unroll
-        for (int m = 0; m < 8; ++m) q[m] = q[m + 2];
+        for (int m = 0; m < 8; ++m) q[m] = q[m + 1];
+        q[8] = lds4(Hp + ro + zo);
+
+        if (y >= ya) {
+            const float *Hy = reinterpret_cast<const float *>(hring + ((y - pf) % SH) * T::HSLOT);
+            const int cs = (y - ya) % SC;
+            const float *Cq = reinterpret_cast<const float *>(cring + (2 * cs) * T::CSLOT);
+            const float *Cv = reinterpret_cast<const float *>(cring + (2 * cs + 1) * T::CSLOT);
+            float ax[4], ay[4], az[4];
+            axis_d2<T>(Hy, ro, zo, q, ax, ay, az);
+            const float4 qo = lds4(Cq + lx * T::TZ + 4 * lz);
+            const float4 vv = lds4(Cv + lx * T::TZ + 4 * lz);
+            const int dy = ABC ? pad_depth(y, a.nyy, a.nb) : -1;
+            float4 out;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const float v = comp(vv, e);
+                const float cv = v * v * a.cvel;
+                const float lap = ax[e] + ay[e] + az[e];
+                const float p0 = comp(q[4], e);
+                float old = comp(qo, e);
+                float d = 1.0f;
+                if constexpr (ABC) {
+                    d = cerjan(b1s, pad_depth(zc + e, a.nzz, a.nb), dx, dy);
+                    old = __fmul_rn(d, old);
+                }
+                float nv = fmaf(cv, lap, 2.0f * p0 - old);
+                if constexpr (ABC) nv = __fmul_rn(d, nv);
+                if (zc + e >= a.nzz - 4) nv = comp(qo, e);
+                set_comp(out, e, nv);
+            }
+            // Source sample t+1 goes into the new field, which is exactly where
+            // the reference adds it at the start of the next step
+            // (src/modeling/modeling.cu:347-348).
+            if (y == src.z && xc == src.y) {
+                const int e = src.x - zc;
+                if (e >= 0 && e < 4 && a.t + 1 < a.nt)
+                    set_comp(out, e, comp(out, e) + a.idh3 * a.wavelet[a.t + 1]);
+            }
+            if (row_ok)
+                *reinterpret_cast<float4 *>(Qshot + y * plane + (long long)xc * a.ldz + zc) = out;
+        }
         __syncthreads();
         if (abort_flag) break;
         if (tid == 0) {
             fence_proxy_async();
-            // planes below ya are only queue sources: free once loaded; the
-            // others once they served as the stencil plane y0 or y1
-            const int last = two ? p + 1 : p;
-            const int h_free = o1 ? y1 : (o0 ? y0 : min(last, ya - 1));
-            const int c_free = o1 ? y1 : (o0 ? y0 : ya - 1);
-            refill(h_free, c_free);
+            if (p < ya) {
+                if (p + SH <= pl) issue_h(p + SH);
+            } else if (y >= ya) {
+                if (y + SH <= pl) issue_h(y + SH);
+                if (y + SC < yb) issue_c(y + SC);
+            }
         }
     }
 
     if (abort_flag && tid == 0) {
         raise_status(kErrTimeout);
-        // Drain copies still in flight into this CTA's shared memory: at most
-        // the newest use of each slot is outstanding.
-        for (int p = max(pf, h_issued - SH + 1); p <= h_issued; ++p)
-            mbar_wait(&hbar[(p - pf) % SH], ((p - pf) / SH) & 1);
-        for (int y = max(ya, c_issued - SC + 1); y <= c_issued; ++y)
-            mbar_wait(&cbar[(y - ya) % SC], ((y - ya) / SC) & 1);
+        // Drain copies still in flight into this CTA's shared memory.
+        for (int p = pf; p <= h_issued; ++p) mbar_wait(&hbar[(p - pf) % SH], ((p - pf) / SH) & 1);
+        for (int y = ya; y <= c_issued; ++y) mbar_wait(&cbar[(y - ya) % SC], ((y - ya) / SC) & 1);
     }
 }
 
@@ -314,7 +293,7 @@ __global__ void __launch_bounds__(T::NT)
                        const __grid_constant__ CUtensorMap mv, const __grid_constant__ CUtensorMap mim,
                        const __grid_constant__ CUtensorMap mil, const BwdArgs a)
 {
-    static_assert(SH >= 6, "planes p-4 .. p+1 are read in one iteration");
+    static_assert(SH >= 5, "plane y needs halo slots y..y+4");
     constexpr int NCF = 5;  // centre fields: Ps, Prold, v, image, illum
     extern __shared__ __align__(128) unsigned char smem[];
     unsigned char *hring = smem;                            // SH x {Psold, Pr}
@@ -370,12 +349,10 @@ __global__ void __launch_bounds__(T::NT)
         tma_load_4d(base + 4 * T::CSLOT, &mil, &cbar[s], z0, x0, y, shot);
         c_issued = y;
     };
-    // slot reuse as in the forward kernel
-    auto refill = [&](int h_free, int c_free) {
-        while (h_issued < pl && h_issued + 1 - SH <= h_free) issue_h(h_issued + 1);
-        while (c_issued < yb - 1 && c_issued + 1 - SC <= c_free) issue_c(c_issued + 1);
-    };
-    if (tid == 0) refill(pf - 1, ya - 1);
+    if (tid == 0) {
+        for (int p = pf; p < pf + SH && p <= pl; ++p) issue_h(p);
+        for (int y = ya; y < ya + SC && y < yb; ++y) issue_c(y);
+    }
 
     const int3 src = make_int3(a.binfo->src[shot][0], a.binfo->src[shot][1], a.binfo->src[shot][2]);
     // Stored field A_{N-t} carried source sample N-t; the exact rebuild adds it back.
@@ -386,125 +363,111 @@ __global__ void __launch_bounds__(T::NT)
     const long long plane = (long long)a.ldz * a.nxx;
     const long long sh_off = (long long)shot * a.vol;
 
-    // One output plane y from the queue windows qs/qr[O..O+8].
-    auto step_plane = [&](auto O_, int y, const float4 (&qs)[10], const float4 (&qr)[10]) {
-        constexpr int O = decltype(O_)::value;
-        const int hy = (y - pf) % SH;
-        const float *Hys = reinterpret_cast<const float *>(hring + (2 * hy) * T::HSLOT);
-        const float *Hyr = reinterpret_cast<const float *>(hring + (2 * hy + 1) * T::HSLOT);
-        const int cs = (y - ya) % SC;
-        const float *C = reinterpret_cast<const float *>(cring + cs * NCF * T::CSLOT);
-        constexpr int CF = T::CSLOT / 4;  // floats per centre slot
-        const int co = lx * T::TZ + 4 * lz;
-        const float4 ps_old = lds4(C + 0 * CF + co);
-        const float4 pr_old = lds4(C + 1 * CF + co);
-        const float4 vv = lds4(C + 2 * CF + co);
-        float4 img = lds4(C + 3 * CF + co);
-        float4 ill = lds4(C + 4 * CF + co);
-
-        float sx[4], sy[4], sz[4];
-        axis_d2<T, O>(Hys, ro, zo, qs, sx, sy, sz);
-        float4 ps_new, pr_new;
+    float4 qs[9], qr[9];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const float v = comp(vv, e);
-            const float v2 = v * v;
-            const float cv = v2 * a.cvel;
-            float sv = fmaf(cv, sx[e] + sy[e] + sz[e], 2.0f * comp(qs[O + 4], e) - comp(ps_old, e));
-            set_comp(ps_new, e, sv);
-        }
-        if (y == src.z && xc == src.y) {
-            const int e = src.x - zc;
-            if (e >= 0 && e < 4) set_comp(ps_new, e, comp(ps_new, e) + scorr);
-        }
-        float rx[4], ry[4], rz[4];
-        axis_d2<T, O>(Hyr, ro, zo, qr, rx, ry, rz);
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const float v = comp(vv, e);
-            const float v2 = v * v;
-            const float cv = v2 * a.cvel;
-            const float prc = comp(qr[O + 4], e);
-            set_comp(pr_new, e, fmaf(cv, rx[e] + ry[e] + rz[e], 2.0f * prc - comp(pr_old, e)));
-            const float psn = comp(ps_new, e);
-            const bool in = zc + e < a.nzz - 4;
-            float im = comp(img, e), il = comp(ill, e);
-            if (in) {
-                il = fmaf(psn, psn, il);
-                if constexpr (GRAD) {
-                    const float lz2 = GRAD_DY ? (sx[e] + sz[e] + sy[e]) : (sx[e] + sz[e]);
-                    im += a.gscale * prc * lz2 * v2;
-                } else {
-                    im = fmaf(psn, prc, im);
-                }
-            } else {
-                set_comp(ps_new, e, comp(ps_old, e));
-                set_comp(pr_new, e, comp(pr_old, e));
-            }
-            set_comp(img, e, im);
-            set_comp(ill, e, il);
-        }
-        if (row_ok) {
-            const long long off = sh_off + y * plane + (long long)xc * a.ldz + zc;
-            *reinterpret_cast<float4 *>(a.Ps + off) = ps_new;
-            *reinterpret_cast<float4 *>(a.Prold + off) = pr_new;
-            *reinterpret_cast<float4 *>(a.image + off) = img;
-            *reinterpret_cast<float4 *>(a.illum + off) = ill;
-        }
-    };
-
-    // Two planes per iteration, as in the forward kernel.
-    float4 qs[10], qr[10];
-#pragma unroll
-    for (int m = 0; m < 10; ++m) {
+    for (int m = 0; m < 9; ++m) {
         qs[m] = make_float4(0.f, 0.f, 0.f, 0.f);
         qr[m] = qs[m];
     }
 
-    for (int p = pf; p <= pl; p += 2) {
-        const bool two = p + 1 <= pl;
-        const int y0 = p - 4, y1 = p - 3;
-        const bool o0 = y0 >= ya, o1 = two && y1 >= ya;
+    for (int p = pf; p <= pl; ++p) {
+        const int y = p - 4;
         bool ok = mbar_wait(&hbar[(p - pf) % SH], ((p - pf) / SH) & 1);
-        if (two) ok = mbar_wait(&hbar[(p + 1 - pf) % SH], ((p + 1 - pf) / SH) & 1) && ok;
-        if (o0) ok = mbar_wait(&cbar[(y0 - ya) % SC], ((y0 - ya) / SC) & 1) && ok;
-        if (o1) ok = mbar_wait(&cbar[(y1 - ya) % SC], ((y1 - ya) / SC) & 1) && ok;
+        if (y >= ya) ok = mbar_wait(&cbar[(y - ya) % SC], ((y - ya) / SC) & 1) && ok;
         if (!ok) abort_flag = 1;
 
-        {
-            const int hs = (p - pf) % SH;
-            qs[8] = lds4(reinterpret_cast<const float *>(hring + (2 * hs) * T::HSLOT) + ro + zo);
-            qr[8] = lds4(reinterpret_cast<const float *>(hring + (2 * hs + 1) * T::HSLOT) + ro + zo);
-        }
-        if (two) {
-            const int hs = (p + 1 - pf) % SH;
-            qs[9] = lds4(reinterpret_cast<const float *>(hring + (2 * hs) * T::HSLOT) + ro + zo);
-            qr[9] = lds4(reinterpret_cast<const float *>(hring + (2 * hs + 1) * T::HSLOT) + ro + zo);
-        }
-        if (o0) step_plane(std::integral_constant<int, 0>{}, y0, qs, qr);
-        if (o1) step_plane(std::integral_constant<int, 1>{}, y1, qs, qr);
+        const int hs = (p - pf) % SH;
+        const float *Hs = reinterpret_cast<const float *>(hring + (2 * hs) * T::HSLOT);
+        const float *Hr = reinterpret_cast<const float *>(hring + (2 * hs + 1) * T::HSLOT);
 #pragma unroll
         for (int m = 0; m < 8; ++m) {
-            qs[m] = qs[m + 2];
-            qr[m] = qr[m + 2];
+            qs[m] = qs[m + 1];
+            qr[m] = qr[m + 1];
+        }
+        qs[8] = lds4(Hs + ro + zo);
+        qr[8] = lds4(Hr + ro + zo);
+
+        if (y >= ya) {
+            const int hy = (y - pf) % SH;
+            const float *Hys = reinterpret_cast<const float *>(hring + (2 * hy) * T::HSLOT);
+            const float *Hyr = reinterpret_cast<const float *>(hring + (2 * hy + 1) * T::HSLOT);
+            const int cs = (y - ya) % SC;
+            const float *C = reinterpret_cast<const float *>(cring + cs * NCF * T::CSLOT);
+            constexpr int CF = T::CSLOT / 4;  // floats per centre slot
+            const int co = lx * T::TZ + 4 * lz;
+            const float4 ps_old = lds4(C + 0 * CF + co);
+            const float4 pr_old = lds4(C + 1 * CF + co);
+            const float4 vv = lds4(C + 2 * CF + co);
+            float4 img = lds4(C + 3 * CF + co);
+            float4 ill = lds4(C + 4 * CF + co);
+
+            float sx[4], sy[4], sz[4];
+            axis_d2<T>(Hys, ro, zo, qs, sx, sy, sz);
+            float4 ps_new, pr_new;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const float v = comp(vv, e);
+                const float v2 = v * v;
+                const float cv = v2 * a.cvel;
+                float s = fmaf(cv, sx[e] + sy[e] + sz[e], 2.0f * comp(qs[4], e) - comp(ps_old, e));
+                set_comp(ps_new, e, s);
+            }
+            if (y == src.z && xc == src.y) {
+                const int e = src.x - zc;
+                if (e >= 0 && e < 4) set_comp(ps_new, e, comp(ps_new, e) + scorr);
+            }
+            float rx[4], ry[4], rz[4];
+            axis_d2<T>(Hyr, ro, zo, qr, rx, ry, rz);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const float v = comp(vv, e);
+                const float v2 = v * v;
+                const float cv = v2 * a.cvel;
+                const float prc = comp(qr[4], e);
+                set_comp(pr_new, e, fmaf(cv, rx[e] + ry[e] + rz[e], 2.0f * prc - comp(pr_old, e)));
+                const float psn = comp(ps_new, e);
+                const bool in = zc + e < a.nzz - 4;
+                float im = comp(img, e), il = comp(ill, e);
+                if (in) {
+                    il = fmaf(psn, psn, il);
+                    if constexpr (GRAD) {
+                        const float lz2 = GRAD_DY ? (sx[e] + sz[e] + sy[e]) : (sx[e] + sz[e]);
+                        im += a.gscale * prc * lz2 * v2;
+                    } else {
+                        im = fmaf(psn, prc, im);
+                    }
+                } else {
+                    set_comp(ps_new, e, comp(ps_old, e));
+                    set_comp(pr_new, e, comp(pr_old, e));
+                }
+                set_comp(img, e, im);
+                set_comp(ill, e, il);
+            }
+            if (row_ok) {
+                const long long off = sh_off + y * plane + (long long)xc * a.ldz + zc;
+                *reinterpret_cast<float4 *>(a.Ps + off) = ps_new;
+                *reinterpret_cast<float4 *>(a.Prold + off) = pr_new;
+                *reinterpret_cast<float4 *>(a.image + off) = img;
+                *reinterpret_cast<float4 *>(a.illum + off) = ill;
+            }
         }
         __syncthreads();
         if (abort_flag) break;
         if (tid == 0) {
             fence_proxy_async();
-            const int last = two ? p + 1 : p;
-            const int h_free = o1 ? y1 : (o0 ? y0 : min(last, ya - 1));
-            const int c_free = o1 ? y1 : (o0 ? y0 : ya - 1);
-            refill(h_free, c_free);
+            if (p < ya) {
+                if (p + SH <= pl) issue_h(p + SH);
+            } else if (y >= ya) {
+                if (y + SH <= pl) issue_h(y + SH);
+                if (y + SC < yb) issue_c(y + SC);
+            }
         }
     }
 
     if (abort_flag && tid == 0) {
         raise_status(kErrTimeout);
-        for (int p = max(pf, h_issued - SH + 1); p <= h_issued; ++p)
-            mbar_wait(&hbar[(p - pf) % SH], ((p - pf) / SH) & 1);
-        for (int y = max(ya, c_issued - SC + 1); y <= c_issued; ++y)
-            mbar_wait(&cbar[(y - ya) % SC], ((y - ya) / SC) & 1);
+        for (int p = pf; p <= h_issued; ++p) mbar_wait(&hbar[(p - pf) % SH], ((p - pf) / SH) & 1);
+        for (int y = ya; y <= c_issued; ++y) mbar_wait(&cbar[(y - ya) % SC], ((y - ya) / SC) & 1);
     }
 }
 
