@@ -387,6 +387,18 @@ __global__ void rbc_blobs_kernel(float *__restrict__ vp, int nzz, int nxx, int n
     }
 }
 
+// Stencil coefficient dt^2 v^2 / dh^2 of every cell, evaluated as
+// (v * v) * cvel exactly as the stencil kernels would, so reading it instead
+// of the velocity changes no result bit.
+__global__ void coeff_kernel(const float *__restrict__ vp, float *__restrict__ out, long long n, float cvel)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+         c += (long long)gridDim.x * blockDim.x) {
+        const float v = vp[c];
+        out[c] = v * v * cvel;
+    }
+}
+
 // Largest |v| in a pitched field restricted to the real cells (CFL check).
 __global__ void max_abs_kernel(const float *__restrict__ v, long long n, int ldz, int nzz,
                                unsigned int *__restrict__ out_bits)

@@ -273,8 +273,11 @@ __global__ void __launch_bounds__(T::NT)
     if (abort_flag && tid == 0) {
         raise_status(kErrTimeout);
         // Drain copies still in flight into this CTA's shared memory.
-        for (int p = pf; p <= h_issued; ++p) mbar_wait(&hbar[(p - pf) % SH], ((p - pf) / SH) & 1);
-        for (int y = ya; y <= c_issued; ++y) mbar_wait(&cbar[(y - ya) % SC], ((y - ya) / SC) & 1);
+        // (only the newest use of each slot can still be in flight)
+        for (int p = max(pf, h_issued - SH + 1); p <= h_issued; ++p)
+            mbar_wait(&hbar[(p - pf) % SH], ((p - pf) / SH) & 1);
+        for (int y = max(ya, c_issued - SC + 1); y <= c_issued; ++y)
+            mbar_wait(&cbar[(y - ya) % SC], ((y - ya) / SC) & 1);
     }
 }
 
@@ -282,7 +285,9 @@ __global__ void __launch_bounds__(T::NT)
 // Fused backward step.
 //   mhs, mhr: halo maps over Psold and Pr
 //   mcs, mcr: centre maps over Ps and Prold (old time levels, overwritten)
-//   mv:       centre map over the velocity slots (shared, or one per shot)
+//   mv:       centre map over the velocity slots (shared, or one per shot);
+//             with the image condition over their stencil coefficient
+//             dt^2 v^2 / dh^2 instead (the gradient condition also needs v^2)
 //   mim, mil: centre maps over the image/gradient and illumination slots
 // GRAD: gradient imaging condition (with GRAD_DY the d2y term is kept).
 // ---------------------------------------------------------------------------
@@ -331,15 +336,13 @@ __global__ void __launch_bounds__(T::NT)
 
     const int pf = ya - 4, pl = yb + 3;
     int h_issued = pf - 1, c_issued = ya - 1;
-    auto issue_h = [&](int p) {
-        const int s = (p - pf) % SH;
+    auto issue_h = [&](int p, int s) {
         mbar_expect_tx(&hbar[s], 2 * T::HALO_BYTES);
         tma_load_4d(hring + (2 * s) * T::HSLOT, &mhs, &hbar[s], z0 - 4, x0 - 4, p, shot);
         tma_load_4d(hring + (2 * s + 1) * T::HSLOT, &mhr, &hbar[s], z0 - 4, x0 - 4, p, shot);
         h_issued = p;
     };
-    auto issue_c = [&](int y) {
-        const int s = (y - ya) % SC;
+    auto issue_c = [&](int y, int s) {
         unsigned char *base = cring + s * NCF * T::CSLOT;
         mbar_expect_tx(&cbar[s], NCF * T::CTR_BYTES);
         tma_load_4d(base + 0 * T::CSLOT, &mcs, &cbar[s], z0, x0, y, shot);
@@ -350,8 +353,8 @@ __global__ void __launch_bounds__(T::NT)
         c_issued = y;
     };
     if (tid == 0) {
-        for (int p = pf; p < pf + SH && p <= pl; ++p) issue_h(p);
-        for (int y = ya; y < ya + SC && y < yb; ++y) issue_c(y);
+        for (int p = pf; p < pf + SH && p <= pl; ++p) issue_h(p, p - pf);
+        for (int y = ya; y < ya + SC && y < yb; ++y) issue_c(y, y - ya);
     }
 
     const int3 src = make_int3(a.binfo->src[shot][0], a.binfo->src[shot][1], a.binfo->src[shot][2]);
@@ -370,13 +373,17 @@ __global__ void __launch_bounds__(T::NT)
         qr[m] = qs[m];
     }
 
+    // Ring positions as counters (no division by the ring depths per plane):
+    // hs, hph = slot and phase parity of halo plane p; hy = slot of plane
+    // y = p - 4; cs, cph = slot and phase parity of centre plane y.
+    int hs = 0, hph = 0, cs = 0, cph = 0;
     for (int p = pf; p <= pl; ++p) {
         const int y = p - 4;
-        bool ok = mbar_wait(&hbar[(p - pf) % SH], ((p - pf) / SH) & 1);
-        if (y >= ya) ok = mbar_wait(&cbar[(y - ya) % SC], ((y - ya) / SC) & 1) && ok;
+        const int hy = hs >= 4 ? hs - 4 : hs + SH - 4;
+        bool ok = mbar_wait(&hbar[hs], hph);
+        if (y >= ya) ok = mbar_wait(&cbar[cs], cph) && ok;
         if (!ok) abort_flag = 1;
 
-        const int hs = (p - pf) % SH;
         const float *Hs = reinterpret_cast<const float *>(hring + (2 * hs) * T::HSLOT);
         const float *Hr = reinterpret_cast<const float *>(hring + (2 * hs + 1) * T::HSLOT);
 #pragma unroll
@@ -388,10 +395,8 @@ __global__ void __launch_bounds__(T::NT)
         qr[8] = lds4(Hr + ro + zo);
 
         if (y >= ya) {
-            const int hy = (y - pf) % SH;
             const float *Hys = reinterpret_cast<const float *>(hring + (2 * hy) * T::HSLOT);
             const float *Hyr = reinterpret_cast<const float *>(hring + (2 * hy + 1) * T::HSLOT);
-            const int cs = (y - ya) % SC;
             const float *C = reinterpret_cast<const float *>(cring + cs * NCF * T::CSLOT);
             constexpr int CF = T::CSLOT / 4;  // floats per centre slot
             const int co = lx * T::TZ + 4 * lz;
@@ -407,8 +412,7 @@ __global__ void __launch_bounds__(T::NT)
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
                 const float v = comp(vv, e);
-                const float v2 = v * v;
-                const float cv = v2 * a.cvel;
+                const float cv = GRAD ? v * v * a.cvel : v;
                 float s = fmaf(cv, sx[e] + sy[e] + sz[e], 2.0f * comp(qs[4], e) - comp(ps_old, e));
                 set_comp(ps_new, e, s);
             }
@@ -421,8 +425,8 @@ __global__ void __launch_bounds__(T::NT)
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
                 const float v = comp(vv, e);
-                const float v2 = v * v;
-                const float cv = v2 * a.cvel;
+                const float v2 = v * v;  // used by the gradient condition only
+                const float cv = GRAD ? v2 * a.cvel : v;
                 const float prc = comp(qr[4], e);
                 set_comp(pr_new, e, fmaf(cv, rx[e] + ry[e] + rz[e], 2.0f * prc - comp(pr_old, e)));
                 const float psn = comp(ps_new, e);
@@ -456,18 +460,29 @@ __global__ void __launch_bounds__(T::NT)
         if (tid == 0) {
             fence_proxy_async();
             if (p < ya) {
-                if (p + SH <= pl) issue_h(p + SH);
+                if (p + SH <= pl) issue_h(p + SH, hs);
             } else if (y >= ya) {
-                if (y + SH <= pl) issue_h(y + SH);
-                if (y + SC < yb) issue_c(y + SC);
+                if (y + SH <= pl) issue_h(y + SH, hy);
+                if (y + SC < yb) issue_c(y + SC, cs);
             }
+        }
+        if (++hs == SH) {
+            hs = 0;
+            hph ^= 1;
+        }
+        if (y >= ya && ++cs == SC) {
+            cs = 0;
+            cph ^= 1;
         }
     }
 
     if (abort_flag && tid == 0) {
         raise_status(kErrTimeout);
-        for (int p = pf; p <= h_issued; ++p) mbar_wait(&hbar[(p - pf) % SH], ((p - pf) / SH) & 1);
-        for (int y = ya; y <= c_issued; ++y) mbar_wait(&cbar[(y - ya) % SC], ((y - ya) / SC) & 1);
+        // (only the newest use of each slot can still be in flight)
+        for (int p = max(pf, h_issued - SH + 1); p <= h_issued; ++p)
+            mbar_wait(&hbar[(p - pf) % SH], ((p - pf) / SH) & 1);
+        for (int y = max(ya, c_issued - SC + 1); y <= c_issued; ++y)
+            mbar_wait(&cbar[(y - ya) % SC], ((y - ya) / SC) & 1);
     }
 }
 
