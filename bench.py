@@ -342,8 +342,9 @@ def run_ours(args, ws, rank, local):
         "data": "synthetic: seeded layered model with Gaussian anomalies, seeded random observed data",
         "config": {
             "workload": (f"{w.name}: padded {ctx.nzz}x{ctx.nxx}x{ctx.nyy}, nt={w.nt}, N={N} steps; "
-                         + ("one shot per step: random boundary + forward + fused backward (3 cell-updates "
-                            "per padded cell per step)" if rtm else "one shot per step: forward modeling")),
+                         + (f"one batch of {B} shots per step, in one launch per time step, each shot through its "
+                            "own new random boundary: forward + fused backward (3 cell-updates per padded cell, "
+                            "time step and shot)" if rtm else "one shot per step: forward modeling")),
             "shots": nsrc, "shots_per_step": B, "shots_per_launch": B, "l2": l2_note,
             "tiles": ctx.tiles(), "parallelism": f"shots/{ws}"},
         "roofline": roof,
