@@ -253,22 +253,28 @@ def run_ours(args, ws, rank, local):
     ms = max_over_ranks(ms_local, ws)
     value = updates_per_step * args.steps * ws / (ms / 1e3) / 1e6
 
-    # roofline of the dominant kernel: the fused backward step (44 B per
-    # cell-step) for RTM, the forward step (16 B per cell-update) for modeling
+    # roofline of the dominant kernel: the fused backward step for RTM (28 B
+    # per cell-step for the four wavefield levels and the stencil coefficient,
+    # plus 16 B for the image and illumination of every cell of the physical
+    # box, the only cells that accumulate), the forward step (16 B per
+    # cell-update) for modeling
     peak, peak_kind = hbm_peak()
-    # per launch: B shots of the padded grid; frac_updated charges only the
-    # cells a launch writes (the outer 4-cell shell is read, never written)
+    # per launch: B shots of the padded grid; frac_updated charges the field
+    # bytes only to the cells a launch writes (the outer 4-cell shell is read,
+    # never written)
+    box = w.nz * w.nx * w.ny
     if rtm:
         kern_ms = timing[1] / args.steps / N
-        per_cell = 44.0
+        bytes_per_launch = (28.0 * cells + 16.0 * box) * B
+        bytes_updated = (28.0 * updated + 16.0 * box) * B
         name = "fd_backward_kernel"
     else:
         kern_ms = timing[0] / args.steps / N
-        per_cell = 16.0
+        bytes_per_launch = 16.0 * cells * B
+        bytes_updated = 16.0 * updated * B
         name = "fd_forward_kernel"
-    bytes_per_launch = per_cell * cells * B
     achieved = bytes_per_launch / (kern_ms / 1e3) / 1e9
-    achieved_upd = per_cell * updated * B / (kern_ms / 1e3) / 1e9
+    achieved_upd = bytes_updated / (kern_ms / 1e3) / 1e9
     traffic = None
     try:
         tr = json.loads(TRAFFIC.read_text())
@@ -282,7 +288,7 @@ def run_ours(args, ws, rank, local):
             "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
             "achieved_updated": round(achieved_upd, 1), "frac_updated": round(achieved_upd / peak, 4),
             "traffic": traffic, "algorithmic_bytes": bytes_per_launch,
-            "algorithmic_bytes_updated": per_cell * updated * B,
+            "algorithmic_bytes_updated": bytes_updated, "accumulated_cells_per_shot": box if rtm else 0,
             "launch_ms": round(kern_ms, 5), "shots_per_launch": B,
             "forward_kernel": {"achieved": round(16.0 * cells * B / (fwd_ms / 1e3) / 1e9, 1),
                                "frac": round(16.0 * cells * B / (fwd_ms / 1e3) / 1e9 / peak, 4),

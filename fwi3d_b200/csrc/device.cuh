@@ -65,6 +65,9 @@ struct BwdArgs {
     float idh3;
     int subtract_src;             // remove the source while rebuilding Ps
     int vel_slots;                // 1: every shot reads velocity slot 0; B: shot s reads slot s
+    int acc_z0, acc_z1;           // box [acc_z0, acc_z1) x [acc_x0, acc_x1) x [acc_y0, acc_y1)
+    int acc_x0, acc_x1;           // of the cells whose image and illumination accumulate;
+    int acc_y0, acc_y1;           // the accumulators of every other cell are neither read nor written
     float *Ps;                    // rebuilt source field (written)
     const float *Psold;           // source field read with the stencil
     float *Prold;                 // adjoint field written

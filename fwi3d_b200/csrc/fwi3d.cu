@@ -677,6 +677,17 @@ BwdLaunch make_bwd(fwi_ctx *c, int n, int tile, int nchunk, bool grad)
     a.idh3 = c->idh3;
     a.subtract_src = (c->p.flags & FWI_FLAG_SUBTRACT_SOURCE) ? 1 : 0;
     a.vel_slots = c->vel_slots;
+    if (c->p.flags & FWI_FLAG_PAD_ACCUMULATE) {  // every updated cell
+        a.acc_z0 = a.acc_x0 = a.acc_y0 = 4;
+        a.acc_z1 = c->nzz - 4;
+        a.acc_x1 = c->nxx - 4;
+        a.acc_y1 = c->nyy - 4;
+    } else {  // the physical box, the only cells that the post-processing reads
+        a.acc_z0 = a.acc_x0 = a.acc_y0 = c->g.nb;
+        a.acc_z1 = c->g.nb + c->g.nz;
+        a.acc_x1 = c->g.nb + c->g.nx;
+        a.acc_y1 = c->g.nb + c->g.ny;
+    }
     a.image = c->acc_img.p;
     a.illum = c->acc_ill.p;
     a.wavelet = c->wavelet.p;

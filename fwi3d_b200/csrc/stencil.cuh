@@ -323,6 +323,11 @@ __global__ void __launch_bounds__(T::NT)
     const int lz = tid % T::TZ4, lx = tid / T::TZ4;
     const int zc = z0 + 4 * lz, xc = x0 + lx;
     const int vshot = a.vel_slots > 1 ? shot : 0;
+    // Accumulator box: a CTA whose tile misses it in z or x, and every plane
+    // outside it in y, moves no accumulator bytes at all.
+    const bool acc_tile = z0 < a.acc_z1 && z0 + T::TZ > a.acc_z0 && x0 < a.acc_x1 && x0 + T::TX > a.acc_x0;
+    const bool acc_row = xc >= a.acc_x0 && xc < a.acc_x1 && zc < a.acc_z1 && zc + 4 > a.acc_z0;
+    auto acc_plane = [&](int y) { return acc_tile && y >= a.acc_y0 && y < a.acc_y1; };
 
     if (tid == 0) {
         abort_flag = 0;
@@ -344,12 +349,15 @@ __global__ void __launch_bounds__(T::NT)
     };
     auto issue_c = [&](int y, int s) {
         unsigned char *base = cring + s * NCF * T::CSLOT;
-        mbar_expect_tx(&cbar[s], NCF * T::CTR_BYTES);
+        const bool acc = acc_plane(y);
+        mbar_expect_tx(&cbar[s], (acc ? NCF : NCF - 2) * T::CTR_BYTES);
         tma_load_4d(base + 0 * T::CSLOT, &mcs, &cbar[s], z0, x0, y, shot);
         tma_load_4d(base + 1 * T::CSLOT, &mcr, &cbar[s], z0, x0, y, shot);
         tma_load_4d(base + 2 * T::CSLOT, &mv, &cbar[s], z0, x0, y, vshot);
-        tma_load_4d(base + 3 * T::CSLOT, &mim, &cbar[s], z0, x0, y, shot);
-        tma_load_4d(base + 4 * T::CSLOT, &mil, &cbar[s], z0, x0, y, shot);
+        if (acc) {
+            tma_load_4d(base + 3 * T::CSLOT, &mim, &cbar[s], z0, x0, y, shot);
+            tma_load_4d(base + 4 * T::CSLOT, &mil, &cbar[s], z0, x0, y, shot);
+        }
         c_issued = y;
     };
     if (tid == 0) {
@@ -403,8 +411,12 @@ __global__ void __launch_bounds__(T::NT)
             const float4 ps_old = lds4(C + 0 * CF + co);
             const float4 pr_old = lds4(C + 1 * CF + co);
             const float4 vv = lds4(C + 2 * CF + co);
-            float4 img = lds4(C + 3 * CF + co);
-            float4 ill = lds4(C + 4 * CF + co);
+            const bool acc = acc_plane(y);
+            float4 img = make_float4(0.f, 0.f, 0.f, 0.f), ill = img;
+            if (acc) {
+                img = lds4(C + 3 * CF + co);
+                ill = lds4(C + 4 * CF + co);
+            }
 
             float sx[4], sy[4], sz[4];
             axis_d2<T>(Hys, ro, zo, qs, sx, sy, sz);
@@ -430,9 +442,14 @@ __global__ void __launch_bounds__(T::NT)
                 const float prc = comp(qr[4], e);
                 set_comp(pr_new, e, fmaf(cv, rx[e] + ry[e] + rz[e], 2.0f * prc - comp(pr_old, e)));
                 const float psn = comp(ps_new, e);
-                const bool in = zc + e < a.nzz - 4;
-                float im = comp(img, e), il = comp(ill, e);
-                if (in) {
+                const int ze = zc + e;
+                if (ze >= a.nzz - 4) {
+                    set_comp(ps_new, e, comp(ps_old, e));
+                    set_comp(pr_new, e, comp(pr_old, e));
+                }
+                // (the box lies inside the updated cells: acc_z1 <= nzz - 4)
+                if (acc && acc_row && ze >= a.acc_z0 && ze < a.acc_z1) {
+                    float im = comp(img, e), il = comp(ill, e);
                     il = fmaf(psn, psn, il);
                     if constexpr (GRAD) {
                         const float lz2 = GRAD_DY ? (sx[e] + sz[e] + sy[e]) : (sx[e] + sz[e]);
@@ -440,19 +457,18 @@ __global__ void __launch_bounds__(T::NT)
                     } else {
                         im = fmaf(psn, prc, im);
                     }
-                } else {
-                    set_comp(ps_new, e, comp(ps_old, e));
-                    set_comp(pr_new, e, comp(pr_old, e));
+                    set_comp(img, e, im);
+                    set_comp(ill, e, il);
                 }
-                set_comp(img, e, im);
-                set_comp(ill, e, il);
             }
             if (row_ok) {
                 const long long off = sh_off + y * plane + (long long)xc * a.ldz + zc;
                 *reinterpret_cast<float4 *>(a.Ps + off) = ps_new;
                 *reinterpret_cast<float4 *>(a.Prold + off) = pr_new;
-                *reinterpret_cast<float4 *>(a.image + off) = img;
-                *reinterpret_cast<float4 *>(a.illum + off) = ill;
+                if (acc && acc_row) {
+                    *reinterpret_cast<float4 *>(a.image + off) = img;
+                    *reinterpret_cast<float4 *>(a.illum + off) = ill;
+                }
             }
         }
         __syncthreads();

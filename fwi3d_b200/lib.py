@@ -25,6 +25,7 @@ BOUNDARY_ABC = 0
 BOUNDARY_RBC = 1
 FLAG_GRAD_DY = 0x1
 FLAG_SUBTRACT_SOURCE = 0x2
+FLAG_PAD_ACCUMULATE = 0x4   # accumulate in the pad too (default: the physical box only)
 
 STATUS_NAMES = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "device allocation failed",
                 4: "device wait timed out", 5: "call out of order", 6: "file could not be opened",

@@ -56,6 +56,15 @@ extern "C" {
                                        src/inversion/inversion.cu:466) */
 #define FWI_FLAG_SUBTRACT_SOURCE 0x2 /* remove the source while rebuilding the forward field
                                        backwards (reference does not, migration.cu:195) */
+#define FWI_FLAG_PAD_ACCUMULATE 0x4  /* accumulate the image / gradient and the illumination
+                                       in the pad as well, as the reference does
+                                       (migration.cu:134-202, inversion.cu:400-468).  Without
+                                       it only the physical box [nb, nb+n) accumulates: the
+                                       only cells that the reference's post-processing reads
+                                       (reduce_boundary in migration.cu:90-97 and
+                                       inversion.cu:142-146), so the image and the gradient
+                                       are the same bit for bit, and the pad accumulators
+                                       keep their values (zero after a reset) */
 
 typedef struct fwi_ctx fwi_ctx;
 

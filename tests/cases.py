@@ -21,6 +21,13 @@ def rel_l2(a, b) -> float:
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
+def interior(a, nb: int) -> np.ndarray:
+    """The physical box of a padded volume: by default the library accumulates
+    images, gradients and illumination there only (the reference's
+    post-processing crops the pad away before it reads them)."""
+    return np.asarray(a)[nb:-nb, nb:-nb, nb:-nb]
+
+
 def indices(w: synth.Workload, nb: int):
     """Flat padded indices of the source(s) and receivers (oracle mapping)."""
     nzz, nxx = w.nz + 2 * nb, w.nx + 2 * nb

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import oracle as orc
-from cases import TOL_GRAD, TOL_IMAGE, TOL_SEIS, context, indices, oracle_wavelet, rel_l2
+from cases import TOL_GRAD, TOL_IMAGE, TOL_SEIS, context, indices, interior, oracle_wavelet, rel_l2
 from fwi3d_b200 import lib, synth
 
 pytestmark = pytest.mark.gpu
@@ -61,10 +61,13 @@ def test_forward_rbc_matches_oracle(small):
     assert err < TOL_SEIS, f"RBC seismogram rel L2 {err:.3e}"
 
 
+@pytest.mark.parametrize("pad", [False, True])
 @pytest.mark.parametrize("grad,with_dy", [(False, False), (True, False), (True, True)])
-def test_backward_matches_oracle(small, grad, with_dy):
+def test_backward_matches_oracle(small, grad, with_dy, pad):
+    """pad: the reference's accumulation over every updated cell; otherwise
+    the physical box accumulates and the pad keeps its zeros."""
     w = small
-    flags = lib.FLAG_GRAD_DY if with_dy else 0
+    flags = (lib.FLAG_GRAD_DY if with_dy else 0) | (lib.FLAG_PAD_ACCUMULATE if pad else 0)
     ctx = context(w, lib.BOUNDARY_RBC, flags=flags)
     ctx.set_velocity(w.vp)
     ctx.apply_random_boundary(kind=1, ratio=0.3, seed=3)
@@ -80,6 +83,11 @@ def test_backward_matches_oracle(small, grad, with_dy):
     _, P, Q, w64, src, rec = _oracle_forward(ctx, w, vpp, abc=False)
     rimg, rill, _, _ = orc.backward(vpp, w.dh, w.dt, w.nt, ctx.tlag, rec, data, P, Q, mode=int(grad),
                                     with_dy=with_dy, w=w64, src=src[0])
+    if not pad:
+        box = np.zeros(img.shape, bool)
+        box[w.nb:-w.nb, w.nb:-w.nb, w.nb:-w.nb] = True
+        assert not img[~box].any() and not ill[~box].any()
+        img, ill, rimg, rill = (interior(a, w.nb) for a in (img, ill, rimg, rill))
     e_img, e_ill = rel_l2(img, rimg), rel_l2(ill, rill)
     tol = TOL_GRAD if grad else TOL_IMAGE
     assert e_img < tol and e_ill < tol, f"image {e_img:.3e} illum {e_ill:.3e}"
@@ -161,7 +169,7 @@ def test_source_subtraction_restores_the_forward_field(small):
     _, P, Q, w64, src, rec = _oracle_forward(ctx, w, vpp, abc=False)
     _, rill, _, _ = orc.backward(vpp, w.dh, w.dt, w.nt, ctx.tlag, rec, data, P, Q, mode=0,
                                  subtract_src=True, w=w64, src=src[0])
-    assert rel_l2(ill, rill) < TOL_IMAGE
+    assert rel_l2(interior(ill, w.nb), interior(rill, w.nb)) < TOL_IMAGE
 
 
 def test_residual_fp64():

@@ -49,7 +49,8 @@ def test_reference_modeling_abc(case):
 @pytest.mark.parametrize("backward", [1, 2])
 def test_reference_backward(case, backward):
     w, params = case
-    ctx = context(w, lib.BOUNDARY_RBC)
+    # the reference's padded accumulators: accumulate in the pad too
+    ctx = context(w, lib.BOUNDARY_RBC, flags=lib.FLAG_PAD_ACCUMULATE)
     ctx.set_velocity(w.vp)
     ctx.apply_random_boundary(kind=0, ratio=60.0, varVp=300.0, seed=5)
     vpp = ctx.get_padded_velocity()
