@@ -68,6 +68,7 @@ struct BwdArgs {
     int acc_z0, acc_z1;           // box [acc_z0, acc_z1) x [acc_x0, acc_x1) x [acc_y0, acc_y1)
     int acc_x0, acc_x1;           // of the cells whose image and illumination accumulate;
     int acc_y0, acc_y1;           // the accumulators of every other cell are neither read nor written
+    int acc_zbox;                 // z extent of the accumulator tiles, from z = floor4(max(z0, acc_z0))
     float *Ps;                    // rebuilt source field (written)
     const float *Psold;           // source field read with the stencil
     float *Prold;                 // adjoint field written

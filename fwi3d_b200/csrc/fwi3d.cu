@@ -658,10 +658,29 @@ BwdLaunch make_bwd(fwi_ctx *c, int n, int tile, int nchunk, bool grad)
     }
     // the gradient condition needs v^2 itself; the image condition only the coefficient
     L.mv = make_map(grad ? c->vp.p : c->vc.p, c->nzz, c->nxx, c->nyy, c->ldz, c->vel_slots, L.k.tz, L.k.tx);
-    L.mim = make_map(c->acc_img.p, c->nzz, c->nxx, c->nyy, c->ldz, n, L.k.tz, L.k.tx);
-    L.mil = make_map(c->acc_ill.p, c->nzz, c->nxx, c->nyy, c->ldz, n, L.k.tz, L.k.tx);
     BwdArgs &a = L.a;
     memset(&a, 0, sizeof a);
+    if (c->p.flags & FWI_FLAG_PAD_ACCUMULATE) {  // every updated cell
+        a.acc_z0 = a.acc_x0 = a.acc_y0 = 4;
+        a.acc_z1 = c->nzz - 4;
+        a.acc_x1 = c->nxx - 4;
+        a.acc_y1 = c->nyy - 4;
+    } else {  // the physical box, the only cells that the post-processing reads
+        a.acc_z0 = a.acc_x0 = a.acc_y0 = c->g.nb;
+        a.acc_z1 = c->g.nb + c->g.nz;
+        a.acc_x1 = c->g.nb + c->g.nx;
+        a.acc_y1 = c->g.nb + c->g.ny;
+    }
+    // z extent of the accumulator tiles: the widest part of a z tile that
+    // reaches the box, from and to float4 boundaries (a multiple of 4 and at
+    // most tz, since every tile starts at a multiple of 4)
+    a.acc_zbox = 4;
+    for (int z0 = 4; z0 < c->nzz - 4; z0 += L.k.tz) {
+        const int lo = std::max(z0, a.acc_z0) & ~3, hi = (std::min(z0 + L.k.tz, a.acc_z1) + 3) & ~3;
+        if (lo < hi) a.acc_zbox = std::max(a.acc_zbox, hi - lo);
+    }
+    L.mim = make_map(c->acc_img.p, c->nzz, c->nxx, c->nyy, c->ldz, n, a.acc_zbox, L.k.tx);
+    L.mil = make_map(c->acc_ill.p, c->nzz, c->nxx, c->nyy, c->ldz, n, a.acc_zbox, L.k.tx);
     a.nzz = c->nzz;
     a.nxx = c->nxx;
     a.nyy = c->nyy;
@@ -677,17 +696,6 @@ BwdLaunch make_bwd(fwi_ctx *c, int n, int tile, int nchunk, bool grad)
     a.idh3 = c->idh3;
     a.subtract_src = (c->p.flags & FWI_FLAG_SUBTRACT_SOURCE) ? 1 : 0;
     a.vel_slots = c->vel_slots;
-    if (c->p.flags & FWI_FLAG_PAD_ACCUMULATE) {  // every updated cell
-        a.acc_z0 = a.acc_x0 = a.acc_y0 = 4;
-        a.acc_z1 = c->nzz - 4;
-        a.acc_x1 = c->nxx - 4;
-        a.acc_y1 = c->nyy - 4;
-    } else {  // the physical box, the only cells that the post-processing reads
-        a.acc_z0 = a.acc_x0 = a.acc_y0 = c->g.nb;
-        a.acc_z1 = c->g.nb + c->g.nz;
-        a.acc_x1 = c->g.nb + c->g.nx;
-        a.acc_y1 = c->g.nb + c->g.ny;
-    }
     a.image = c->acc_img.p;
     a.illum = c->acc_ill.p;
     a.wavelet = c->wavelet.p;

@@ -328,6 +328,11 @@ __global__ void __launch_bounds__(T::NT)
     const bool acc_tile = z0 < a.acc_z1 && z0 + T::TZ > a.acc_z0 && x0 < a.acc_x1 && x0 + T::TX > a.acc_x0;
     const bool acc_row = xc >= a.acc_x0 && xc < a.acc_x1 && zc < a.acc_z1 && zc + 4 > a.acc_z0;
     auto acc_plane = [&](int y) { return acc_tile && y >= a.acc_y0 && y < a.acc_y1; };
+    // Accumulator tiles cover z in [za, za + acc_zbox) only: the part of the
+    // tile's z range that reaches the box, widened to float4 boundaries (the
+    // TMA start stays 16-byte aligned).
+    const int za = max(z0, a.acc_z0) & ~3;
+    const int acc_bytes = a.acc_zbox * T::TX * 4;
 
     if (tid == 0) {
         abort_flag = 0;
@@ -350,13 +355,13 @@ __global__ void __launch_bounds__(T::NT)
     auto issue_c = [&](int y, int s) {
         unsigned char *base = cring + s * NCF * T::CSLOT;
         const bool acc = acc_plane(y);
-        mbar_expect_tx(&cbar[s], (acc ? NCF : NCF - 2) * T::CTR_BYTES);
+        mbar_expect_tx(&cbar[s], (NCF - 2) * T::CTR_BYTES + (acc ? 2 * acc_bytes : 0));
         tma_load_4d(base + 0 * T::CSLOT, &mcs, &cbar[s], z0, x0, y, shot);
         tma_load_4d(base + 1 * T::CSLOT, &mcr, &cbar[s], z0, x0, y, shot);
         tma_load_4d(base + 2 * T::CSLOT, &mv, &cbar[s], z0, x0, y, vshot);
         if (acc) {
-            tma_load_4d(base + 3 * T::CSLOT, &mim, &cbar[s], z0, x0, y, shot);
-            tma_load_4d(base + 4 * T::CSLOT, &mil, &cbar[s], z0, x0, y, shot);
+            tma_load_4d(base + 3 * T::CSLOT, &mim, &cbar[s], za, x0, y, shot);
+            tma_load_4d(base + 4 * T::CSLOT, &mil, &cbar[s], za, x0, y, shot);
         }
         c_issued = y;
     };
@@ -413,9 +418,10 @@ __global__ void __launch_bounds__(T::NT)
             const float4 vv = lds4(C + 2 * CF + co);
             const bool acc = acc_plane(y);
             float4 img = make_float4(0.f, 0.f, 0.f, 0.f), ill = img;
-            if (acc) {
-                img = lds4(C + 3 * CF + co);
-                ill = lds4(C + 4 * CF + co);
+            if (acc && acc_row) {  // then za <= zc and zc + 4 <= za + acc_zbox
+                const int ao = lx * a.acc_zbox + (zc - za);
+                img = lds4(C + 3 * CF + ao);
+                ill = lds4(C + 4 * CF + ao);
             }
 
             float sx[4], sy[4], sz[4];
