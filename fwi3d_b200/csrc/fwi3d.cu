@@ -283,6 +283,11 @@ struct fwi_ctx {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaEvent_t ev[4] = {};
+    // host data of back-propagation: copied and transposed on copy_stream
+    // while the forward pass runs; ev_free marks the buffers free, ev_data
+    // the data ready
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_free = nullptr, ev_data = nullptr;
     float fwd_ms = 0, bwd_ms = 0;
     long long launches = 0;
     std::string err;
@@ -831,10 +836,10 @@ void seis_to_fortran(fwi_ctx *c, int R, float *dst)
 }
 
 // Fortran per shot [R][nt] at src (device) -> data_tm [nt][R].
-void data_from_fortran(fwi_ctx *c, int R, const float *src)
+void data_from_fortran(fwi_ctx *c, int R, const float *src, cudaStream_t st = nullptr)
 {
     dim3 grid((c->p.nt + 31) / 32, (R + 31) / 32);
-    transpose_kernel<<<grid, dim3(32, 8), 0, c->stream>>>(src, R, c->p.nt, c->data_tm.p);
+    transpose_kernel<<<grid, dim3(32, 8), 0, st ? st : c->stream>>>(src, R, c->p.nt, c->data_tm.p);
     CK(cudaGetLastError());
     ++c->launches;
 }
@@ -912,12 +917,21 @@ void migrate_impl(fwi_ctx *c, const int *shots, int nshots, const float *data, b
         update_coeff(c);
         const int R = t.info.R;
         const size_t cnt = (size_t)c->p.nt * R;
+        bool data_on_side = false;
         if (R) {
             if (data_is_device) {
                 data_from_fortran(c, R, data + off);
             } else {
-                CK(cudaMemcpyAsync(c->raw.p, data + off, cnt * sizeof(float), cudaMemcpyHostToDevice, c->stream));
-                data_from_fortran(c, R, c->raw.p);
+                // Host data: the forward pass does not read it, so its copy and
+                // transpose run beside that pass, once everything queued so far
+                // (the previous batch's use of raw and data_tm) is done.
+                CK(cudaEventRecord(c->ev_free, c->stream));
+                CK(cudaStreamWaitEvent(c->copy_stream, c->ev_free, 0));
+                CK(cudaMemcpyAsync(c->raw.p, data + off, cnt * sizeof(float), cudaMemcpyHostToDevice,
+                                   c->copy_stream));
+                data_from_fortran(c, R, c->raw.p, c->copy_stream);
+                CK(cudaEventRecord(c->ev_data, c->copy_stream));
+                data_on_side = true;
             }
         }
         start_forward(c, n);
@@ -927,6 +941,7 @@ void migrate_impl(fwi_ctx *c, const int *shots, int nshots, const float *data, b
         CK(cudaMemsetAsync(c->Rf[0].p, 0, bytes, c->stream));
         CK(cudaMemsetAsync(c->Rf[1].p, 0, bytes, c->stream));
         Graph &gb = time_loop_graph(c, grad ? 3 : 2, c->B);
+        if (data_on_side) CK(cudaStreamWaitEvent(c->stream, c->ev_data, 0));
         run_graph(c, gb);
         check_status(c);
         float ms = 0;
@@ -1333,6 +1348,9 @@ int fwi_create(const fwi_grid *grid, const fwi_params *params, fwi_ctx **out)
         CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
         c->own_stream = true;
         for (auto &e : c->ev) CK(cudaEventCreate(&e));
+        CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&c->ev_free, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&c->ev_data, cudaEventDisableTiming));
         make_wavelet(c);
         c->nsteps = c->tlag + c->p.nt;
         make_b1d(c);
@@ -1385,6 +1403,9 @@ int fwi_destroy(fwi_ctx *c)
     c->blob_cache.drain();
     for (auto &e : c->ev)
         if (e) cudaEventDestroy(e);
+    if (c->ev_free) cudaEventDestroy(c->ev_free);
+    if (c->ev_data) cudaEventDestroy(c->ev_data);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return FWI_OK;
