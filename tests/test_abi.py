@@ -30,6 +30,20 @@ def test_binding_covers_the_header():
     assert set(declared_functions()) == set(lib.SIGNATURES)
 
 
+def test_binding_constants_match_the_header():
+    """FWI_FLAG_*, FWI_BOUNDARY_* and the status codes have the header's values
+    in the Python binding."""
+    text = HEADER.read_text()
+    macros = {k: int(v, 0) for k, v in re.findall(r"#define\s+(FWI_[A-Z0-9_]+)\s+(0x[0-9a-fA-F]+|\d+)", text)}
+    for name, value in macros.items():
+        if name.startswith(("FWI_FLAG_", "FWI_BOUNDARY_")):
+            assert getattr(lib, name[len("FWI_"):]) == value, name
+        if name.startswith("FWI_ERR_") or name == "FWI_OK":
+            assert value == 0 or value in lib.STATUS_NAMES, name
+    flags = [v for k, v in macros.items() if k.startswith("FWI_FLAG_")]
+    assert len(flags) == 3 and len(set(flags)) == 3 and all(f & (f - 1) == 0 for f in flags)
+
+
 def test_status_strings():
     so = lib.load()
     assert so.fwi_status_string(0) == b"ok"
