@@ -109,6 +109,6 @@ def test_learned_step_is_kept_only_when_its_measured_misfit_is_at_most_the_plain
     assert all(h["choice"] == "plain" for h in h_bad[:-1])
     assert h_bad[-1]["misfit"] == h_plain[-1]["misfit"]
     for h, nxt in zip(h_good[:-1], h_good[1:]):
-        # the judge compares measured misfits, and the next iterate is the winner
+        # the accept rule compares measured misfits, and the next iterate is the winner
         assert (h["choice"] == "learned") == (h["f_learned"] <= h["f_plain"])
         assert nxt["misfit"] == min(h["f_learned"], h["f_plain"])

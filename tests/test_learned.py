@@ -43,7 +43,7 @@ def test_learned_step_beats_plain_fwi_on_held_out_models(trained):
                         log=lambda *a: None)
         assert hp[0]["misfit"] == hl[0]["misfit"]
         for h, nxt in zip(hl[:-1], hl[1:]):
-            # the judge: the plain step's measured misfit, no slack
+            # the accept rule: the plain step's measured misfit, no slack
             assert (h["choice"] == "learned") == (h["f_learned"] <= h["f_plain"])
             assert nxt["misfit"] == min(h["f_learned"], h["f_plain"])
         ratios.append(hl[-1]["misfit"] / hp[-1]["misfit"])
