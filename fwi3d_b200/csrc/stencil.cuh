@@ -26,7 +26,9 @@
 //     tile of plane y, y neighbours from a 9-deep register queue fed with the
 //     centre of plane y+4.
 //   - Centre-only fields (old time level, velocity, accumulators) arrive as
-//     TZ x TX tiles in a second ring of SC slots.
+//     TZ x TX tiles in a second ring of SC slots; the accumulators only
+//     where the tile meets the box of accumulated cells, and then only over
+//     the z range that meets it.
 //   - One elected thread issues every TMA copy; completion is tracked with
 //     mbarriers whose waits are bounded (kWaitLimitNs) and report through
 //     g_status instead of hanging.
@@ -288,7 +290,9 @@ __global__ void __launch_bounds__(T::NT)
 //   mv:       centre map over the velocity slots (shared, or one per shot);
 //             with the image condition over their stencil coefficient
 //             dt^2 v^2 / dh^2 instead (the gradient condition also needs v^2)
-//   mim, mil: centre maps over the image/gradient and illumination slots
+//   mim, mil: maps over the image/gradient and illumination slots, with a box
+//             of acc_zbox x TX cells (the widest z range of a tile that meets
+//             the accumulated box)
 // GRAD: gradient imaging condition (with GRAD_DY the d2y term is kept).
 // ---------------------------------------------------------------------------
 template <class T, int SH, int SC, bool GRAD, bool GRAD_DY>
