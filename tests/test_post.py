@@ -30,6 +30,25 @@ def test_oracle_post_processing_is_finite_without_illumination():
     assert zmax == 0.0 and np.all(z == 0.0)
 
 
+def test_oracle_post_processing_reads_only_the_physical_box():
+    """The reference crops the pad away before it reads the accumulators
+    (src/migration/migration.cu:90-97, src/inversion/inversion.cu:142-146), so
+    accumulators whose pad is zero (the library's default, which accumulates
+    over the physical box only) give the same image and gradient bit for bit."""
+    rng = np.random.default_rng(3)
+    shape = (NY + 2 * NB, NX + 2 * NB, NZ + 2 * NB)
+    img = rng.standard_normal(shape)
+    ill = rng.uniform(0.5, 2.0, shape)
+    box = np.zeros(shape, bool)
+    box[NB:-NB, NB:-NB, NB:-NB] = True
+    img_box, ill_box = np.where(box, img, 0.0), np.where(box, ill, 0.0)
+    assert np.array_equal(orc.rtm_post(img, ill, NZ, NX, NY, NB, DH), orc.rtm_post(img_box, ill_box, NZ, NX, NY, NB, DH))
+    for zmask in (0.0, 30.0):
+        g, gmax = orc.gradient_post(img, ill, NZ, NX, NY, NB, DH, zmask)
+        gb, gbmax = orc.gradient_post(img_box, ill_box, NZ, NX, NY, NB, DH, zmask)
+        assert np.array_equal(g, gb) and gmax == gbmax
+
+
 @pytest.mark.gpu
 def test_library_post_processing_matches_the_oracle_without_illumination():
     import torch
